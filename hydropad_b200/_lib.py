@@ -1,0 +1,98 @@
+"""ctypes binding of libhydropad_b200.so (the C ABI in include/hydropad_b200.h).
+
+The library is the only compute path: if it is missing this module raises
+at import time instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB_PATH
+
+HP_OK = 0
+HP_ERR = {
+    -1: "HP_ERR_ARG", -2: "HP_ERR_CUDA", -3: "HP_ERR_OOM", -4: "HP_ERR_NEWTON", -5: "HP_ERR_NAN",
+    -6: "HP_ERR_NEGATIVE_STATE", -7: "HP_ERR_NOT_ATTACHED", -8: "HP_ERR_STATE_MISMATCH", -9: "HP_ERR_NO_DEVICE",
+}
+HP_PREC_FP64 = 0
+HP_PREC_MIXED = 1
+
+
+class HpParams(C.Structure):
+    _fields_ = [
+        ("ngridx", C.c_int), ("ngridy", C.c_int), ("ngridz", C.c_int), ("nbound", C.c_int),
+        ("gamma", C.c_double), ("cour", C.c_double), ("ca", C.c_double), ("eta1", C.c_double),
+        ("eta2", C.c_double), ("dmax", C.c_double), ("flatvalue", C.c_double), ("mingradflat", C.c_double),
+        ("dtinit", C.c_double), ("tstop", C.c_double),
+        ("cosmo", C.c_int), ("expand_zero_old", C.c_int),
+        ("a_start", C.c_double), ("dt_cap", C.c_double),
+        ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+class HpScalars(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "dt", "rdtath", "at", "dat", "rat", "ath", "dath",
+        "t", "told", "thalf", "dtold", "atnew", "datnew", "velmax")] + [
+        ("nstep", C.c_int), ("pad", C.c_int)]
+
+
+class HydroError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        name = HP_ERR.get(code, str(code))
+        msg = lib().hp_strerror(code).decode()
+        super().__init__(f"{what}: {name} ({msg})" if what else f"{name} ({msg})")
+
+
+EXPORTS = (
+    "hp_init", "hp_finalize", "hp_set_scalars", "hp_get_scalars", "hp_attach_state", "hp_sync_to_host",
+    "hp_download_state", "hp_ppmsolver", "hp_ppm_lxlylz", "hp_speed", "hp_timedet", "hp_evolve",
+    "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count",
+)
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m hydropad_b200.build` (needs nvcc)")
+    L = C.CDLL(LIB_PATH)
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    cp = C.c_void_p
+    L.hp_init.argtypes = [C.POINTER(HpParams), C.POINTER(cp)]
+    L.hp_finalize.argtypes = [cp]
+    L.hp_set_scalars.argtypes = [cp, C.POINTER(HpScalars)]
+    L.hp_get_scalars.argtypes = [cp, C.POINTER(HpScalars)]
+    L.hp_attach_state.argtypes = [cp, dp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.hp_sync_to_host.argtypes = [cp]
+    L.hp_download_state.argtypes = [cp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.hp_ppmsolver.argtypes = [cp, dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, ip, ip, ip]
+    L.hp_ppm_lxlylz.argtypes = [cp, C.c_int]
+    L.hp_speed.argtypes = [cp, dp]
+    L.hp_timedet.argtypes = [cp, C.c_double]
+    L.hp_evolve.argtypes = [cp, C.c_int, C.c_int]
+    L.hp_synchronize.argtypes = [cp]
+    L.hp_stream.argtypes = [cp]
+    L.hp_stream.restype = cp
+    L.hp_device_fields.argtypes = [cp] + [C.POINTER(dp)] * 5
+    L.hp_strerror.argtypes = [C.c_int]
+    L.hp_strerror.restype = C.c_char_p
+    L.hp_launch_count.argtypes = [cp]
+    L.hp_launch_count.restype = C.c_longlong
+    for name in EXPORTS:
+        if name not in ("hp_stream", "hp_strerror", "hp_launch_count"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != HP_OK:
+        raise HydroError(rc, what)

@@ -1,0 +1,168 @@
+"""Host-side mirror of the reference's hydro-step interface.
+
+One :class:`Hydro` object is one box whose state lives in HBM.  Method names
+follow the reference routines they replace:
+
+=====================  =====================================================
+``ppmsolver(nd)``      hydro/ppmsolver.F90:1-467 (one directional sweep)
+``ppm_lxlylz(nrot)``   hydro/ppm_lxlylz.F90:1-223 (+ exchange_mesh)
+``speed()``            hydropad/speed.F90:2-59
+``timedet(velmax)``    hydropad/functions.F90:61-210
+``evolve(nsteps)``     hydro part of evolve_sys.F90:30-130, looped as in
+                       main.F90:200-221
+``attach_state``       the `!$acc update device` of ppmsolver.F90:95
+``sync_to_host``       the `!$acc update host` of ppm_lxlylz.F90:20
+=====================  =====================================================
+
+Host arrays are REAL(8) Fortran-order ``(nx, ny, nz)`` with ``nbound`` ghost
+layers, the reference's module arrays (hydropad/matrix.F90:10).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .params import HydroParams
+
+
+def _dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.f_contiguous, "state arrays must be Fortran-ordered float64"
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Hydro:
+    """One box advanced by the fused B200 sweeps."""
+
+    def __init__(self, params: HydroParams, precision: str = "fp64", device: int = 0):
+        self.params = params
+        self.precision = precision
+        p = L.HpParams()
+        p.ngridx, p.ngridy, p.ngridz = (int(v) for v in params.shape)
+        p.nbound = params.nbound
+        p.gamma = params.gamma
+        p.cour = params.cour
+        p.ca = params.ca
+        p.eta1 = params.eta1
+        p.eta2 = params.eta2
+        p.dmax = params.dmax
+        p.flatvalue = params.flatvalue
+        p.mingradflat = params.mingradflat
+        p.dtinit = params.dtinit
+        p.tstop = params.tstop
+        p.cosmo = 1 if params.cosmo else 0
+        p.expand_zero_old = 1 if params.expand_zero_old else 0
+        p.a_start = params.a_start
+        p.dt_cap = params.dt_cap
+        p.precision = {"fp64": L.HP_PREC_FP64, "mixed": L.HP_PREC_MIXED}[precision]
+        p.device = device
+        self._ctx = C.c_void_p()
+        L.check(L.lib().hp_init(C.byref(p), C.byref(self._ctx)), "hp_init")
+        self._host = None
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            L.lib().hp_finalize(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state --------------------------------------------------------------
+    def attach_state(self, p3d, rho3d, vx3d, vy3d, vz3d):
+        """Upload ghosted Fortran-order host arrays; the device copy becomes
+        the working state (the arrays are kept for :meth:`sync_to_host`)."""
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (p3d, rho3d, vx3d, vy3d, vz3d)]
+        nx, ny, nz = arrs[0].shape
+        nb = (nx - self.params.shape[0]) // 2
+        L.check(L.lib().hp_attach_state(self._ctx, *[_dptr(a) for a in arrs], None, nx, ny, nz, nb),
+                "hp_attach_state")
+        self._host = arrs
+        return arrs
+
+    def sync_to_host(self):
+        L.check(L.lib().hp_sync_to_host(self._ctx), "hp_sync_to_host")
+        return self._host
+
+    def download(self, nbound: int | None = None):
+        """Return (p, rho, vx, vy, vz) as new ghosted Fortran arrays."""
+        nb = self.params.nbound if nbound is None else nbound
+        shp = tuple(int(n) + 2 * nb for n in self.params.shape)
+        out = [np.zeros(shp, dtype=np.float64, order="F") for _ in range(5)]
+        L.check(L.lib().hp_download_state(self._ctx, *[_dptr(a) for a in out], *shp, nb), "hp_download_state")
+        return out
+
+    # -- the hydro step ----------------------------------------------------------
+    def ppmsolver(self, ndirection: int):
+        """One sweep through the drop-in entry point (Fortran by-reference
+        argument list; the host arrays identify the attached state)."""
+        a = self._host
+        nx, ny, nz = (C.c_int(v) for v in a[0].shape)
+        nb = C.c_int(self.params.nbound)
+        nd = C.c_int(int(ndirection))
+        rc = L.lib().hp_ppmsolver(self._ctx, *[_dptr(x) for x in a], None, None, None,
+                                  C.byref(nx), C.byref(ny), C.byref(nz), C.byref(nb), C.byref(nd))
+        L.check(rc, "hp_ppmsolver")
+
+    def ppm_lxlylz(self, nrot: int):
+        L.check(L.lib().hp_ppm_lxlylz(self._ctx, int(nrot)), "hp_ppm_lxlylz")
+        L.check(L.lib().hp_synchronize(self._ctx), "hp_ppm_lxlylz")
+
+    def speed(self) -> float:
+        v = C.c_double()
+        L.check(L.lib().hp_speed(self._ctx, C.byref(v)), "hp_speed")
+        return v.value
+
+    def timedet(self, velmax: float):
+        L.check(L.lib().hp_timedet(self._ctx, float(velmax)), "hp_timedet")
+
+    def start_with_cfl(self):
+        """Take the first step's dt from the CFL condition of the attached
+        state instead of dtinit: the clock is put back to the initial time
+        (told) and speed + timedet run once (the configurations' choice)."""
+        s = self.get_scalars()
+        s.t = s.told
+        self.set_scalars(s)
+        self.timedet(self.speed())
+
+    def evolve(self, nsteps: int, graph: bool = True):
+        L.check(L.lib().hp_evolve(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve")
+
+    def evolve_async(self, nsteps: int, graph: bool = True):
+        """Enqueue nsteps without the final status read (for timing loops);
+        call :meth:`synchronize` afterwards."""
+        L.check(L.lib().hp_evolve(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve")
+
+    def synchronize(self):
+        L.check(L.lib().hp_synchronize(self._ctx), "hp_synchronize")
+
+    # -- scalars ------------------------------------------------------------------
+    def get_scalars(self) -> L.HpScalars:
+        s = L.HpScalars()
+        L.check(L.lib().hp_get_scalars(self._ctx, C.byref(s)), "hp_get_scalars")
+        return s
+
+    def set_scalars(self, s: L.HpScalars):
+        L.check(L.lib().hp_set_scalars(self._ctx, C.byref(s)), "hp_set_scalars")
+
+    def stream_handle(self) -> int:
+        return int(L.lib().hp_stream(self._ctx) or 0)
+
+    def launch_count(self) -> int:
+        return int(L.lib().hp_launch_count(self._ctx))
+
+    def device_field_ptrs(self):
+        ptrs = [C.POINTER(C.c_double)() for _ in range(5)]
+        L.check(L.lib().hp_device_fields(self._ctx, *[C.byref(p) for p in ptrs]), "hp_device_fields")
+        return [C.cast(p, C.c_void_p).value for p in ptrs]

@@ -1,0 +1,71 @@
+"""Build recipe of the CUDA library (libhydropad_b200.so, in-tree).
+
+Every kernel is compiled for sm_100a only.  The FP64 kernels are compiled
+without multiply-add contraction (--fmad=false) so that they round like the
+reference's scalar Fortran; the mixed-precision kernels and the host code use
+the default.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+BUILD_DIR = os.path.join(ROOT, "_build")
+LIB_NAME = "libhydropad_b200.so"
+LIB_PATH = os.path.join(HERE, LIB_NAME)
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
+SOURCES = [
+    ("hp_kernels_fp64.cu", ["--fmad=false"]),
+    ("hp_kernels_mixed.cu", []),
+    ("hp_api.cu", []),
+]
+HEADERS = ["hp_physics.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_launch.h"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build hydropad_b200")
+
+
+def _mtime(p: str) -> float:
+    return os.path.getmtime(p) if os.path.exists(p) else -1.0
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    """Compile stale objects and link the shared library; return its path."""
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    nvcc = _nvcc()
+    deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "hydropad_b200.h")]
+    newest_dep = max(_mtime(d) for d in deps)
+    objs = []
+    relink = force or not os.path.exists(LIB_PATH)
+    for src, extra in SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD_DIR, src.replace(".cu", ".o"))
+        objs.append(o)
+        if force or _mtime(o) < max(_mtime(s), newest_dep):
+            cmd = [nvcc, *ARCH, *COMMON, *extra, "-c", s, "-o", o]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+                print(" ".join(cmd), file=sys.stderr)
+            subprocess.run(cmd, check=True)
+            relink = True
+    if relink or _mtime(LIB_PATH) < max(_mtime(o) for o in objs):
+        cmd = [nvcc, *ARCH, "-shared", "-o", LIB_PATH, *objs]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

@@ -1,0 +1,510 @@
+// hp_api.cu -- C ABI of the B200 PPM hydro step (include/hydropad_b200.h).
+//
+// Host-side mirror of the reference's call structure: initialize_parameters
+// (time init), ppmsolver / ppm_lxlylz (sweeps), speed + timedet (CFL), and
+// evolve_sys' hydro loop, over one box whose state stays resident in HBM.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/hydropad_b200.h"
+#include "hp_device.cuh"
+#include "hp_launch.h"
+
+namespace hp {
+int launch_sweep_fp64(const Box& b, int axis, int bslot, int flags, cudaStream_t st);
+int launch_sweep_mixed(const Box& b, int axis, int bslot, int flags, cudaStream_t st);
+size_t sweep_smem_bytes_fp64(int axis);
+size_t sweep_smem_bytes_mixed(int axis);
+
+int launch_sweep(const Box& b, int axis, int bslot, int flags, int precision, cudaStream_t st) {
+    return precision == HP_PREC_MIXED ? launch_sweep_mixed(b, axis, bslot, flags, st)
+                                      : launch_sweep_fp64(b, axis, bslot, flags, st);
+}
+size_t sweep_smem_bytes(int axis, int precision) {
+    return precision == HP_PREC_MIXED ? sweep_smem_bytes_mixed(axis) : sweep_smem_bytes_fp64(axis);
+}
+}  // namespace hp
+
+struct hp_ctx {
+    hp_params prm;
+    int dev;
+    cudaStream_t stream;
+    hp::Box box;
+    hp::DevCtl* ctl_pinned;   // host mirror for reads
+    long long sweep_count;    // selects the rho-bound slot
+    long long nstep_host;     // host mirror of the step counter (selects nrot)
+    const double* host[5];    // attached host arrays (ghosted, Fortran order)
+    int hnx, hny, hnz, hnb;
+    bool attached;
+    cudaGraphExec_t graph[6][3];
+    int graph_kernels[6][3];
+    long long launches;
+};
+
+namespace {
+
+// REAL(4) literals used by the time initialisation (initialize_parameters.F90)
+constexpr double kC0P010 = 0.009999999776482582;  // 0.010
+constexpr double kTwo3 = 0.6666666865348816;      // 2.0/3.0
+constexpr double kMThird = -0.3333333432674408;   // -1.0/3.0
+
+int cuda_fail(cudaError_t e) {
+    if (e == cudaSuccess) return HP_OK;
+    if (e == cudaErrorMemoryAllocation) return HP_ERR_OOM;
+    return HP_ERR_CUDA;
+}
+#define HP_CUDA(x)                                       \
+    do {                                                 \
+        cudaError_t e_ = (x);                            \
+        if (e_ != cudaSuccess) return cuda_fail(e_);     \
+    } while (0)
+
+int status_to_err(unsigned st) {
+    if (st & hp::kStatNewton) return HP_ERR_NEWTON;
+    if (st & hp::kStatNaN) return HP_ERR_NAN;
+    if (st & hp::kStatNegative) return HP_ERR_NEGATIVE_STATE;
+    return HP_OK;
+}
+
+// initialize_parameters.F90:133-205 on a host DevCtl.
+void init_time(const hp_params& p, hp::DevCtl& c) {
+    if (p.cosmo) {
+        double at = p.a_start;
+        const double tin = pow(at, 1.5);
+        c.told = tin;
+        c.s.dt = kC0P010 * tin;
+        c.dtold = c.s.dt;
+        c.t = tin + c.s.dt;
+        c.thalf = c.told + c.s.dt / 2.0;
+        c.s.at = pow(c.told, kTwo3);
+        c.atnew = pow(c.t, kTwo3);
+        c.s.dat = kTwo3 * pow(c.told, kMThird);
+        c.s.ath = pow(c.told + c.s.dt / 2.0, kTwo3);
+        c.s.dath = kTwo3 * pow(c.thalf, kMThird);
+        c.datnew = kTwo3 * pow(c.t, kMThird);
+        c.s.rat = 1.0 / c.s.at;
+        c.s.rdtath = c.s.dt / c.s.ath;
+    } else {
+        c.told = 0.0;
+        c.s.dt = p.dtinit;
+        c.dtold = c.s.dt;
+        c.t = c.told + c.s.dt;
+        c.s.at = 1.0;
+        c.atnew = 1.0;
+        c.s.dat = 0.0;
+        c.s.ath = 1.0;
+        c.s.dath = 0.0;
+        c.datnew = 0.0;
+        c.s.rat = 1.0;
+        c.s.rdtath = c.s.dt / c.s.ath;
+        c.thalf = c.told + 0.5 * c.s.dt;
+    }
+}
+
+int copy_ctl_to_device(hp_ctx* x) {
+    HP_CUDA(cudaMemcpyAsync(x->box.ctl, x->ctl_pinned, sizeof(hp::DevCtl), cudaMemcpyHostToDevice, x->stream));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return HP_OK;
+}
+int copy_ctl_to_host(hp_ctx* x) {
+    HP_CUDA(cudaMemcpyAsync(x->ctl_pinned, x->box.ctl, sizeof(hp::DevCtl), cudaMemcpyDeviceToHost, x->stream));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return HP_OK;
+}
+
+// Ghosted Fortran host array <-> dense device interior.
+cudaMemcpy3DParms host_dev_parms(const double* host, double* dev, const hp_ctx* x, int nxg, int nyg, int nb,
+                                 bool to_device) {
+    cudaMemcpy3DParms prm;
+    memset(&prm, 0, sizeof prm);
+    cudaPitchedPtr hp_ = make_cudaPitchedPtr((void*)host, (size_t)nxg * sizeof(double), (size_t)nxg, (size_t)nyg);
+    cudaPitchedPtr dp_ = make_cudaPitchedPtr((void*)dev, (size_t)x->box.nx * sizeof(double), (size_t)x->box.nx,
+                                             (size_t)x->box.ny);
+    cudaPos hpos = make_cudaPos((size_t)nb * sizeof(double), (size_t)nb, (size_t)nb);
+    cudaPos dpos = make_cudaPos(0, 0, 0);
+    if (to_device) {
+        prm.srcPtr = hp_; prm.srcPos = hpos; prm.dstPtr = dp_; prm.dstPos = dpos;
+        prm.kind = cudaMemcpyHostToDevice;
+    } else {
+        prm.srcPtr = dp_; prm.srcPos = dpos; prm.dstPtr = hp_; prm.dstPos = hpos;
+        prm.kind = cudaMemcpyDeviceToHost;
+    }
+    prm.extent = make_cudaExtent((size_t)x->box.nx * sizeof(double), (size_t)x->box.ny, (size_t)x->box.nz);
+    return prm;
+}
+
+// Periodic ghost layers of one host array (exchange_mesh.F90 with one rank).
+void fill_ghosts(double* a, int nx, int ny, int nz, int nb) {
+#define IX(i, j, k) ((size_t)(i) + (size_t)nx * ((size_t)(j) + (size_t)ny * (size_t)(k)))
+    for (int k = 0; k < nb; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                a[IX(i, j, k)] = a[IX(i, j, nz - 2 * nb + k)];
+                a[IX(i, j, nz - nb + k)] = a[IX(i, j, k + nb)];
+            }
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < nb; ++j)
+            for (int i = 0; i < nx; ++i) {
+                a[IX(i, j, k)] = a[IX(i, ny - 2 * nb + j, k)];
+                a[IX(i, ny - nb + j, k)] = a[IX(i, j + nb, k)];
+            }
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nb; ++i) {
+                a[IX(i, j, k)] = a[IX(nx - 2 * nb + i, j, k)];
+                a[IX(nx - nb + i, j, k)] = a[IX(i + nb, j, k)];
+            }
+#undef IX
+}
+
+// One fused sweep on the resident state.
+int do_sweep(hp_ctx* x, int axis, int flags) {
+    const int bslot = (int)(x->sweep_count % 3);
+    int n = hp::launch_peak_prepass(x->box, axis, bslot, x->stream);
+    if (n < 0) return HP_ERR_CUDA;
+    x->launches += n;
+    n = hp::launch_sweep(x->box, axis, bslot, flags, x->prm.precision, x->stream);
+    if (n < 0) return HP_ERR_CUDA;
+    x->launches += n;
+    x->sweep_count += 1;
+    return HP_OK;
+}
+
+const int kOrder[6][3] = {{0, 1, 2}, {2, 1, 0}, {1, 2, 0}, {0, 2, 1}, {2, 0, 1}, {1, 0, 2}};  // ppm_lxlylz.F90
+
+// One evolve_sys step on the device: three sweeps (the first snapshots the
+// state for expand, the last applies expand and accumulates velmax) and
+// timedet.  Returns the number of kernels or a negative error.
+int enqueue_step(hp_ctx* x, int nrot) {
+    const bool cosmo = x->prm.cosmo != 0;
+    int kern = 0;
+    for (int s = 0; s < 3; ++s) {
+        int flags = 0;
+        if (s == 0) {
+            flags |= hp::kFlagResetSpeed;
+            if (cosmo && !x->prm.expand_zero_old) flags |= hp::kFlagSnapshot;
+        }
+        if (s == 2) {
+            flags |= hp::kFlagSpeed;
+            if (cosmo) flags |= hp::kFlagExpand | (x->prm.expand_zero_old ? hp::kFlagExpandZeroOld : 0);
+        }
+        const long long before = x->launches;
+        const int rc = do_sweep(x, kOrder[nrot - 1][s], flags);
+        if (rc != HP_OK) return rc;
+        kern += (int)(x->launches - before);
+    }
+    if (hp::launch_timedet(x->box, 1, x->stream) < 0) return HP_ERR_CUDA;
+    x->launches += 1;
+    return kern + 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hp_strerror(int code) {
+    switch (code) {
+        case HP_OK: return "ok";
+        case HP_ERR_ARG: return "invalid argument";
+        case HP_ERR_CUDA: return "CUDA runtime error";
+        case HP_ERR_OOM: return "device out of memory";
+        case HP_ERR_NEWTON: return "Riemann Newton iteration did not converge in 100 iterations";
+        case HP_ERR_NAN: return "NaN in the updated state";
+        case HP_ERR_NEGATIVE_STATE: return "non-positive density or pressure in the updated state";
+        case HP_ERR_NOT_ATTACHED: return "no state attached";
+        case HP_ERR_STATE_MISMATCH: return "host arrays are not the attached state";
+        case HP_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
+    }
+    return "unknown error";
+}
+
+int hp_init(const hp_params* p, hp_ctx** out) {
+    if (!p || !out) return HP_ERR_ARG;
+    *out = nullptr;
+    if (p->ngridx < 8 || p->ngridy < 8 || p->ngridz < 8 || p->nbound < 3) return HP_ERR_ARG;
+    if (p->precision != HP_PREC_FP64 && p->precision != HP_PREC_MIXED) return HP_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= p->device || p->device < 0) return HP_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    HP_CUDA(cudaGetDeviceProperties(&prop, p->device));
+    if (prop.major != 10) return HP_ERR_NO_DEVICE;
+    HP_CUDA(cudaSetDevice(p->device));
+
+    hp_ctx* x = new hp_ctx();
+    memset(x, 0, sizeof(*x));
+    x->prm = *p;
+    x->dev = p->device;
+    x->box.nx = p->ngridx;
+    x->box.ny = p->ngridy;
+    x->box.nz = p->ngridz;
+    const size_t n = (size_t)p->ngridx * p->ngridy * p->ngridz;
+    int rc = HP_OK;
+    auto fail = [&](int code) {
+        hp_finalize(x);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(HP_ERR_CUDA);
+    for (int q = 0; q < 5; ++q)
+        if ((rc = cuda_fail(cudaMalloc(&x->box.f[q], n * sizeof(double)))) != HP_OK) return fail(rc);
+    if (p->cosmo && !p->expand_zero_old)
+        for (int q = 0; q < 4; ++q)
+            if ((rc = cuda_fail(cudaMalloc(&x->box.snap[q], n * sizeof(double)))) != HP_OK) return fail(rc);
+    if ((rc = cuda_fail(cudaMalloc(&x->box.peak, n * sizeof(double)))) != HP_OK) return fail(rc);
+    if ((rc = cuda_fail(cudaMalloc(&x->box.ctl, sizeof(hp::DevCtl)))) != HP_OK) return fail(rc);
+    if ((rc = cuda_fail(cudaMallocHost(&x->ctl_pinned, sizeof(hp::DevCtl)))) != HP_OK) return fail(rc);
+
+    // derived constants, initialize_parameters.F90:23-24,63-69
+    hp::Consts& k = x->box.k;
+    const int nmax = p->ngridx > p->ngridy ? (p->ngridx > p->ngridz ? p->ngridx : p->ngridz)
+                                            : (p->ngridy > p->ngridz ? p->ngridy : p->ngridz);
+    k.dx = 1.0 / (double)nmax;
+    k.rdx = 1.0 / k.dx;
+    k.gamma = p->gamma;
+    k.rgamma = 1.0 / p->gamma;
+    k.gamma1 = (p->gamma + 1.0) / (p->gamma - 1.0);
+    k.rgamma1 = 1.0 / (p->gamma - 1.0);
+    k.m = (p->gamma - 1.0) / (2.0 * p->gamma);
+    k.rm = 1.0 / k.m;
+    k.gf = (p->gamma + 1.0) / (2.0 * p->gamma);
+    k.mingradflat = p->mingradflat;
+    k.flatvalue = p->flatvalue;
+    k.dmax = p->dmax;
+    k.eta1 = p->eta1;
+    k.eta2 = p->eta2;
+
+    hp::DevCtl& c = *x->ctl_pinned;
+    memset(&c, 0, sizeof c);
+    init_time(*p, c);
+    c.tstop = p->tstop;
+    c.cosmo = p->cosmo;
+    c.cour = p->cour;
+    c.ca = p->ca;
+    c.dx = k.dx;
+    c.dt_cap = p->dt_cap;
+    c.nstep = 1;
+    for (int s = 0; s < 3; ++s) {
+        c.rho_key[s][0] = hp::kKeyPosInf;
+        c.rho_key[s][1] = hp::kKeyNegInf;
+    }
+    x->nstep_host = 1;
+    if ((rc = copy_ctl_to_device(x)) != HP_OK) return fail(rc);
+    // zero the state so that a sweep before any attach reads defined memory
+    for (int q = 0; q < 5; ++q)
+        if ((rc = cuda_fail(cudaMemsetAsync(x->box.f[q], 0, n * sizeof(double), x->stream))) != HP_OK)
+            return fail(rc);
+    if ((rc = cuda_fail(cudaStreamSynchronize(x->stream))) != HP_OK) return fail(rc);
+    *out = x;
+    return HP_OK;
+}
+
+int hp_finalize(hp_ctx* x) {
+    if (!x) return HP_OK;
+    cudaSetDevice(x->dev);
+    if (x->stream) cudaStreamSynchronize(x->stream);
+    for (int r = 0; r < 6; ++r)
+        for (int s = 0; s < 3; ++s)
+            if (x->graph[r][s]) cudaGraphExecDestroy(x->graph[r][s]);
+    for (int q = 0; q < 5; ++q) cudaFree(x->box.f[q]);
+    for (int q = 0; q < 4; ++q) cudaFree(x->box.snap[q]);
+    cudaFree(x->box.peak);
+    cudaFree(x->box.ctl);
+    if (x->ctl_pinned) cudaFreeHost(x->ctl_pinned);
+    if (x->stream) cudaStreamDestroy(x->stream);
+    delete x;
+    return HP_OK;
+}
+
+int hp_set_scalars(hp_ctx* x, const hp_scalars* s) {
+    if (!x || !s) return HP_ERR_ARG;
+    int rc = copy_ctl_to_host(x);
+    if (rc != HP_OK) return rc;
+    hp::DevCtl& c = *x->ctl_pinned;
+    c.s.dt = s->dt; c.s.rdtath = s->rdtath; c.s.at = s->at; c.s.dat = s->dat; c.s.rat = s->rat;
+    c.s.ath = s->ath; c.s.dath = s->dath;
+    c.t = s->t; c.told = s->told; c.thalf = s->thalf; c.dtold = s->dtold; c.atnew = s->atnew;
+    c.datnew = s->datnew; c.velmax = s->velmax; c.nstep = s->nstep;
+    c.done = (c.told < c.tstop) ? 0 : 1;
+    x->nstep_host = s->nstep;
+    return copy_ctl_to_device(x);
+}
+
+int hp_get_scalars(hp_ctx* x, hp_scalars* s) {
+    if (!x || !s) return HP_ERR_ARG;
+    int rc = copy_ctl_to_host(x);
+    if (rc != HP_OK) return rc;
+    const hp::DevCtl& c = *x->ctl_pinned;
+    s->dt = c.s.dt; s->rdtath = c.s.rdtath; s->at = c.s.at; s->dat = c.s.dat; s->rat = c.s.rat;
+    s->ath = c.s.ath; s->dath = c.s.dath;
+    s->t = c.t; s->told = c.told; s->thalf = c.thalf; s->dtold = c.dtold; s->atnew = c.atnew;
+    s->datnew = c.datnew; s->velmax = c.velmax; s->nstep = c.nstep; s->pad = 0;
+    return HP_OK;
+}
+
+int hp_attach_state(hp_ctx* x, const double* p3d, const double* rho3d, const double* vx3d, const double* vy3d,
+                    const double* vz3d, const double* gforce, int nx, int ny, int nz, int nbound) {
+    if (!x || !p3d || !rho3d || !vx3d || !vy3d || !vz3d) return HP_ERR_ARG;
+    if (gforce) return HP_ERR_ARG;  // gravity source not supported: configs run without gravity
+    if (nbound < 0 || nx != x->box.nx + 2 * nbound || ny != x->box.ny + 2 * nbound || nz != x->box.nz + 2 * nbound)
+        return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    const double* src[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
+    for (int q = 0; q < 5; ++q) {
+        cudaMemcpy3DParms prm = host_dev_parms(src[q], x->box.f[q], x, nx, ny, nbound, true);
+        HP_CUDA(cudaMemcpy3DAsync(&prm, x->stream));
+        x->host[q] = src[q];
+    }
+    x->hnx = nx; x->hny = ny; x->hnz = nz; x->hnb = nbound;
+    x->attached = true;
+    x->sweep_count = 0;
+    const int n = hp::launch_bounds(x->box, 0, x->stream);
+    if (n < 0) return HP_ERR_CUDA;
+    x->launches += n;
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return HP_OK;
+}
+
+int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, double* vy3d, double* vz3d, int nx,
+                      int ny, int nz, int nbound) {
+    if (!x || !p3d || !rho3d || !vx3d || !vy3d || !vz3d) return HP_ERR_ARG;
+    if (nbound < 0 || nx != x->box.nx + 2 * nbound || ny != x->box.ny + 2 * nbound || nz != x->box.nz + 2 * nbound)
+        return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    double* dst[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
+    for (int q = 0; q < 5; ++q) {
+        cudaMemcpy3DParms prm = host_dev_parms(dst[q], x->box.f[q], x, nx, ny, nbound, false);
+        HP_CUDA(cudaMemcpy3DAsync(&prm, x->stream));
+    }
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    if (nbound > 0)
+        for (int q = 0; q < 5; ++q) fill_ghosts(dst[q], nx, ny, nz, nbound);
+    return HP_OK;
+}
+
+int hp_sync_to_host(hp_ctx* x) {
+    if (!x) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    return hp_download_state(x, (double*)x->host[0], (double*)x->host[1], (double*)x->host[2], (double*)x->host[3],
+                             (double*)x->host[4], x->hnx, x->hny, x->hnz, x->hnb);
+}
+
+int hp_ppmsolver(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, double* vy3d, double* vz3d, double* cho3d,
+                 double* nes3d, const double* gforce, const int* nx, const int* ny, const int* nz,
+                 const int* nbound, const int* ndirection) {
+    (void)cho3d;
+    (void)nes3d;
+    if (!x || !nx || !ny || !nz || !nbound || !ndirection) return HP_ERR_ARG;
+    if (gforce) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    if (*ndirection < 1 || *ndirection > 3) return HP_ERR_ARG;
+    if (*nx != x->hnx || *ny != x->hny || *nz != x->hnz || *nbound != x->hnb) return HP_ERR_STATE_MISMATCH;
+    const double* given[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
+    for (int q = 0; q < 5; ++q)
+        if (given[q] != x->host[q]) return HP_ERR_STATE_MISMATCH;
+    HP_CUDA(cudaSetDevice(x->dev));
+    int rc = do_sweep(x, *ndirection - 1, 0);
+    if (rc != HP_OK) return rc;
+    return hp_synchronize(x);
+}
+
+int hp_ppm_lxlylz(hp_ctx* x, int nrot) {
+    if (!x || nrot < 1 || nrot > 6) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    HP_CUDA(cudaSetDevice(x->dev));
+    for (int s = 0; s < 3; ++s) {
+        int rc = do_sweep(x, kOrder[nrot - 1][s], 0);
+        if (rc != HP_OK) return rc;
+    }
+    return HP_OK;
+}
+
+int hp_speed(hp_ctx* x, double* velmax) {
+    if (!x || !velmax) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    if (hp::launch_speed(x->box, x->stream) < 0) return HP_ERR_CUDA;
+    x->launches += 1;
+    unsigned long long bits = 0;
+    HP_CUDA(cudaMemcpyAsync(&bits, &x->box.ctl->velmax_key, sizeof bits, cudaMemcpyDeviceToHost, x->stream));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    memcpy(velmax, &bits, sizeof(double));
+    return HP_OK;
+}
+
+int hp_timedet(hp_ctx* x, double velmax) {
+    if (!x) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    unsigned long long bits;
+    memcpy(&bits, &velmax, sizeof bits);
+    HP_CUDA(cudaMemcpyAsync(&x->box.ctl->velmax_key, &bits, sizeof bits, cudaMemcpyHostToDevice, x->stream));
+    if (hp::launch_timedet(x->box, 0, x->stream) < 0) return HP_ERR_CUDA;
+    x->launches += 1;
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return HP_OK;
+}
+
+int hp_evolve(hp_ctx* x, int nsteps, int use_graph) {
+    if (!x || nsteps < 0) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    HP_CUDA(cudaSetDevice(x->dev));
+    for (int it = 0; it < nsteps; ++it) {
+        const long long nstep = x->nstep_host;
+        int nrot = (int)(nstep % 6) + 1;  // evolve_sys.F90:30-31
+        if (nstep == 1) nrot = 1;
+        const int slot = (int)(x->sweep_count % 3);
+        if (!use_graph) {
+            const int n = enqueue_step(x, nrot);
+            if (n < 0) return n;
+        } else {
+            cudaGraphExec_t& g = x->graph[nrot - 1][slot];
+            if (!g) {
+                cudaGraph_t graph;
+                const long long sc0 = x->sweep_count, l0 = x->launches;
+                HP_CUDA(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+                const int n = enqueue_step(x, nrot);
+                cudaError_t ce = cudaStreamEndCapture(x->stream, &graph);
+                if (n < 0) return n;
+                HP_CUDA(ce);
+                HP_CUDA(cudaGraphInstantiate(&g, graph, 0));
+                cudaGraphDestroy(graph);
+                x->graph_kernels[nrot - 1][slot] = n;
+                x->sweep_count = sc0;  // the capture did not execute anything
+                x->launches = l0;
+            }
+            HP_CUDA(cudaGraphLaunch(g, x->stream));
+            x->sweep_count += 3;
+            x->launches += x->graph_kernels[nrot - 1][slot];
+        }
+        x->nstep_host += 1;
+    }
+    return hp_synchronize(x);
+}
+
+int hp_synchronize(hp_ctx* x) {
+    if (!x) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    unsigned st = 0;
+    HP_CUDA(cudaMemcpyAsync(&st, &x->box.ctl->status, sizeof st, cudaMemcpyDeviceToHost, x->stream));
+    HP_CUDA(cudaMemsetAsync(&x->box.ctl->status, 0, sizeof st, x->stream));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return status_to_err(st);
+}
+
+void* hp_stream(hp_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+int hp_device_fields(hp_ctx* x, double** p, double** rho, double** vx, double** vy, double** vz) {
+    if (!x) return HP_ERR_ARG;
+    if (p) *p = x->box.f[0];
+    if (rho) *rho = x->box.f[1];
+    if (vx) *vx = x->box.f[2];
+    if (vy) *vy = x->box.f[3];
+    if (vz) *vz = x->box.f[4];
+    return HP_OK;
+}
+
+long long hp_launch_count(hp_ctx* x) { return x ? x->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,228 @@
+// hp_kernels_fp64.cu -- FP64 sweep instantiations and the small per-step
+// kernels (rho bounds, CFL speed, timedet, density-peak pre-pass).
+//
+// Compiled with --fmad=false: every FP64 operation rounds once, like the
+// reference's scalar Fortran, so the FP64 path reproduces the oracle to the
+// last bit except where CUDA's pow differs from the host libm by an ulp.
+#include <cuda_runtime.h>
+
+#include "hp_device.cuh"
+#include "hp_launch.h"
+#include "hp_physics.cuh"
+#include "hp_sweep.cuh"
+
+namespace hp {
+
+// Sweep tile shapes: x walks 32-cell rows of 8 pencils, y/z walk 8-cell
+// columns of 32 neighbouring pencils.
+constexpr int kPx = 8, kTx = 32, kRingX = 64;
+constexpr int kPyz = 32, kTyz = 8, kRingYZ = 16;
+
+template <int AXIS, int P, int T, int RING, class Policy>
+static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
+    SweepArgs a;
+    // permute velocities into (normal, transverse1, transverse2) of this
+    // sweep (ppmsolver.F90:105-107, 227-229, 355-357)
+    a.f[0] = b.f[0];
+    a.f[1] = b.f[1];
+    if (AXIS == 0) { a.f[2] = b.f[2]; a.f[3] = b.f[3]; a.f[4] = b.f[4]; }
+    if (AXIS == 1) { a.f[2] = b.f[3]; a.f[3] = b.f[2]; a.f[4] = b.f[4]; }
+    if (AXIS == 2) { a.f[2] = b.f[4]; a.f[3] = b.f[3]; a.f[4] = b.f[2]; }
+    for (int q = 0; q < 4; ++q) a.snap[q] = b.snap[q];
+    a.peak = b.peak;
+    a.ctl = b.ctl;
+    a.k = b.k;
+    a.nx = b.nx; a.ny = b.ny; a.nz = b.nz;
+    a.nsweep = AXIS == 0 ? b.nx : (AXIS == 1 ? b.ny : b.nz);
+    a.npencil = AXIS == 0 ? (long long)b.ny * b.nz : (AXIS == 1 ? (long long)b.nx * b.nz : (long long)b.nx * b.ny);
+    a.bslot = bslot;
+    a.flags = flags;
+    const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy>);
+    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return -1;
+        attr_set = true;
+    }
+    const long long grid = (a.npencil + P - 1) / P;
+    kern<<<(unsigned)grid, P * T, smem, st>>>(a);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+int launch_sweep_fp64(const Box& b, int axis, int bslot, int flags, cudaStream_t st) {
+    switch (axis) {
+        case 0: return launch_sweep_t<0, kPx, kTx, kRingX, PolicyFP64>(b, bslot, flags, st);
+        case 1: return launch_sweep_t<1, kPyz, kTyz, kRingYZ, PolicyFP64>(b, bslot, flags, st);
+        case 2: return launch_sweep_t<2, kPyz, kTyz, kRingYZ, PolicyFP64>(b, bslot, flags, st);
+    }
+    return -1;
+}
+
+size_t sweep_smem_bytes_fp64(int axis) {
+    if (axis == 0) return sizeof(SweepSmem<0, kPx, kTx, kRingX, PolicyFP64>);
+    return sizeof(SweepSmem<1, kPyz, kTyz, kRingYZ, PolicyFP64>);
+}
+
+// ---------------------------------------------------------------------------
+// rho bounds of the resident state into slot `slot`; the other two slots are
+// reset.  Feeds the density-peak test of the next sweep.
+// ---------------------------------------------------------------------------
+__global__ void bounds_reset_kernel(DevCtl* c, int slot) {
+    for (int s = 0; s < 3; ++s) {
+        c->rho_key[s][0] = kKeyPosInf;
+        c->rho_key[s][1] = kKeyNegInf;
+    }
+    (void)slot;
+}
+
+__global__ void bounds_kernel(const double* __restrict__ rho, long long n, DevCtl* c, int slot) {
+    __shared__ unsigned long long red[128];
+    unsigned long long kmin = kKeyPosInf, kmax = 0ULL;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long kk = dkey(rho[i]);
+        kmin = kk < kmin ? kk : kmin;
+        kmax = kk > kmax ? kk : kmax;
+    }
+    block_flush(kmin, kmax, 0ULL, 0u, &c->rho_key[slot][0], &c->rho_key[slot][1], nullptr, &c->status, red);
+}
+
+int launch_bounds(const Box& b, int slot, cudaStream_t st) {
+    const long long n = (long long)b.nx * b.ny * b.nz;
+    bounds_reset_kernel<<<1, 1, 0, st>>>(b.ctl, slot);
+    bounds_kernel<<<296, 256, 0, st>>>(b.f[1], n, b.ctl, slot);
+    return cudaPeekAtLastError() == cudaSuccess ? 2 : -1;
+}
+
+// ---------------------------------------------------------------------------
+// speed.F90:17-31: velmax over the resident state (accumulator zeroed first).
+// ---------------------------------------------------------------------------
+__global__ void speed_kernel(const double* __restrict__ p, const double* __restrict__ rho,
+                             const double* __restrict__ vx, const double* __restrict__ vy,
+                             const double* __restrict__ vz, long long n, double gamma, DevCtl* c) {
+    __shared__ unsigned long long red[128];
+    unsigned long long kvel = 0ULL;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double vs = sqrt(gamma * p[i] / rho[i]);
+        double vm = fabs(vx[i]) + vs;
+        vm = fmax2(vm, fabs(vy[i]) + vs);
+        vm = fmax2(vm, fabs(vz[i]) + vs);
+        const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
+        kvel = kb > kvel ? kb : kvel;
+    }
+    block_flush(kKeyPosInf, 0ULL, kvel, 0u, nullptr, nullptr, &c->velmax_key, &c->status, red);
+}
+
+int launch_speed(const Box& b, cudaStream_t st) {
+    const long long n = (long long)b.nx * b.ny * b.nz;
+    if (cudaMemsetAsync(&b.ctl->velmax_key, 0, sizeof(unsigned long long), st) != cudaSuccess) return -1;
+    speed_kernel<<<296, 256, 0, st>>>(b.f[0], b.f[1], b.f[2], b.f[3], b.f[4], n, b.k.gamma, b.ctl);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+// ---------------------------------------------------------------------------
+// timedet (functions.F90:61-94) / timedet_cosmo (functions.F90:97-210, EdS)
+// on the device control block, with velmax from the accumulator.  Advances
+// the step counter (when `advance`: the end of an evolve_sys step) and
+// raises `done` when told reaches tstop (main.F90:200).
+// ---------------------------------------------------------------------------
+constexpr double kC0P1 = 0.10000000149011612;   // 0.1 (functions.F90:80,155)
+constexpr double kTwo3 = 0.6666666865348816;    // 2.0/3.0 as REAL(4)
+constexpr double kMThird = -0.3333333432674408; // -1.0/3.0 as REAL(4)
+
+__global__ void timedet_kernel(DevCtl* c, int advance) {
+    if (c->done) return;
+    const double velmax = __longlong_as_double((long long)c->velmax_key);
+    c->velmax = velmax;
+    if (!c->cosmo) {
+        c->s.at = 1.0;
+        c->s.ath = 1.0;
+        c->s.dat = 0.0;
+        c->told = c->t;
+        c->dtold = c->s.dt;
+        const double rdtc = velmax / (c->cour * c->dx);
+        if (velmax == 0.0) c->s.dt = kC0P1;
+        else c->s.dt = 1.0 / rdtc;
+        c->t = c->t + c->s.dt;
+        if (c->t > c->tstop) {
+            c->t = c->tstop;
+            c->s.dt = c->t - c->told;
+        }
+        const double dth = 0.5 * c->s.dt;
+        c->thalf = c->told + dth;
+        c->s.rdtath = c->s.dt / c->s.ath;
+    } else {
+        c->told = c->t;
+        c->dtold = c->s.dt;
+        const double rdt = c->nstep > 1 ? 5.0 / (6.0 * c->s.dt) : 0.0;
+        c->s.at = pow(c->t, kTwo3);
+        c->s.dat = kTwo3 * pow(c->t, kMThird);
+        const double dta = pow((1.0 + c->ca) * c->s.at, 1.5) - c->t;
+        c->s.rat = 1.0 / c->s.at;
+        const double rdtc = velmax / (c->cour * c->dx * c->s.at);
+        double dt = 1.0 / fmax2(rdt, rdtc);
+        dt = fmin2(dt, dta);
+        if (dt >= 10.0) dt = kC0P1;
+        if (c->dt_cap > 0.0) dt = fmin2(dt, c->dt_cap);
+        c->s.dt = dt;
+        c->t = c->t + c->s.dt;
+        if (c->t > c->tstop) {
+            c->t = c->tstop;
+            c->s.dt = c->t - c->told;
+        }
+        const double dth = 0.5 * c->s.dt;
+        c->thalf = c->told + dth;
+        c->atnew = pow(c->t, kTwo3);
+        c->s.ath = pow(c->thalf, kTwo3);
+        c->s.dath = kTwo3 * pow(c->thalf, kMThird);
+        c->datnew = kTwo3 * pow(c->t, kMThird);
+        c->s.rdtath = c->s.dt / c->s.ath;
+    }
+    if (advance) c->nstep += 1;
+    if (!(c->told < c->tstop)) c->done = 1;
+}
+
+int launch_timedet(const Box& b, int advance, cudaStream_t st) {
+    timedet_kernel<<<1, 1, 0, st>>>(b.ctl, advance);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+// ---------------------------------------------------------------------------
+// Density-peak pre-pass for y/z sweeps.  The reference gathers the peak test
+// with the x-index slot in every direction (ppmsolver.F90:251-252 for y,
+// :379-380 for z): for the y face (x, y, z) it reads rho3d(y-3..y, x, z) and
+// vy3d(y-2..y-1, x, z); for the z face (x, y, z) rho3d(z-3..z, y, x) and
+// vz3d.  Those cells belong to other pencils, which the in-place sweep
+// updates concurrently, so the values are evaluated here on the pre-sweep
+// state.  Indices wrap periodically (identical to the reference's ghost
+// reads for cubic boxes).  Runs only when the rho bounds admit a peak.
+// ---------------------------------------------------------------------------
+__global__ void peak_prepass_kernel(const double* __restrict__ rho, const double* __restrict__ vn, double* peak,
+                                    int nx, int ny, int nz, int axis, double dmax, const DevCtl* c, int bslot) {
+    const double rmin0 = dkey_decode(c->rho_key[bslot][0]);
+    const double rmax0 = dkey_decode(c->rho_key[bslot][1]);
+    if (!(rmax0 > dmax * rmin0) || c->done) return;
+    const long long n = (long long)nx * ny * nz;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % nx);
+        const int y = (int)((i / nx) % ny);
+        const int z = (int)(i / ((long long)nx * ny));
+        // (face index along the sweep, row index y', plane index z') of the
+        // x-row that the reference reads
+        int f, yy, zz;
+        if (axis == 1) { f = y; yy = x % ny; zz = z; }
+        else { f = z; yy = y; zz = x % nz; }
+        const long long row = (long long)nx * (yy + (long long)ny * zz);
+        auto at = [&](int o) { int xi = ((f + o) % nx + nx) % nx; return row + xi; };
+        peak[i] = peak_value(rho[at(-3)], rho[at(-2)], rho[at(-1)], rho[at(0)], vn[at(-2)], vn[at(-1)], dmax);
+    }
+}
+
+int launch_peak_prepass(const Box& b, int axis, int bslot, cudaStream_t st) {
+    if (axis == 0 || b.peak == nullptr) return 0;
+    const double* vn = axis == 1 ? b.f[3] : b.f[4];
+    peak_prepass_kernel<<<592, 256, 0, st>>>(b.f[1], vn, b.peak, b.nx, b.ny, b.nz, axis, b.k.dmax, b.ctl, bslot);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+}  // namespace hp

@@ -1,0 +1,30 @@
+// hp_launch.h -- host-side launch interface between the C ABI and the
+// kernels (internal; not part of the public header).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "hp_device.cuh"
+
+namespace hp {
+
+// One box resident on the device.
+struct Box {
+    double* f[5];      // p, rho, vx, vy, vz (natural order), dense (nx,ny,nz), x fastest
+    double* snap[4];   // step-start p, vx, vy, vz (cosmo expand), or null
+    double* peak;      // density-peak scratch for y/z sweeps (nx*ny*nz), or null
+    DevCtl* ctl;       // device control block
+    Consts k;
+    int nx, ny, nz;
+};
+
+// Launches return the number of kernels launched (>= 0) or -1 on a launch error.
+int launch_sweep(const Box& b, int axis, int bslot, int flags, int precision, cudaStream_t st);
+int launch_peak_prepass(const Box& b, int axis, int bslot, cudaStream_t st);
+int launch_bounds(const Box& b, int slot, cudaStream_t st);
+int launch_speed(const Box& b, cudaStream_t st);
+int launch_timedet(const Box& b, int advance, cudaStream_t st);
+
+// Shared memory a sweep needs (bytes), for the API's capacity checks.
+size_t sweep_smem_bytes(int axis, int precision);
+
+}  // namespace hp

@@ -1,0 +1,419 @@
+// hp_sweep.cuh -- the fused directional PPM sweep (one kernel per axis).
+//
+// Replaces the three OpenACC regions of one ppmsolver call
+// (hydro/ppmsolver.F90:96-160 x, :214-288 y, :342-416 z) and the ghost
+// exchange that follows it (hydro/ppm_lxlylz.F90:20-21):
+//
+//   R1 order2interp (flatten + parabolas + characteristic tracing),
+//   R2 riemannsolver (exact Riemann problem, Newton for p*),
+//   R3 integrate (conservative update + dual energy)
+//
+// run back to back on the same cells with every intermediate in shared
+// memory.  The state is updated in place and read/written exactly once per
+// sweep (5 fields x 8 B in + out = 80 B per cell).
+//
+// Work decomposition.  A CTA owns P whole pencils along the sweep axis and
+// walks them with a sliding window of T cells per iteration.  Each cell's
+// quantities are computed exactly once (the reference evaluates every
+// parabola twice, once per adjacent face) and handed to neighbours through
+// ring buffers of RING cells:
+//
+//   load   cell e                      state ring
+//   A      cell e-1: ajside slopes, dda second difference of rho, the
+//          flattening flag of the pair (e-1, e)          -> A ring
+//   B      cell e-3: flat, parabolas of p, rho, u, v, w, characteristic
+//          tracing -> left state of face e-2 (ls ring), right state of
+//          face e-3 (registers)
+//   C      face e-3: Riemann problem                     -> face ring
+//   D      cell e-4: update from faces e-4 and e-3, store
+//
+// Periodicity is a wrap of the pencil index: the walk starts at cell -4
+// (= N-4) and ends at N+3; the original values of cells 0..2, which the
+// walk re-reads at its end after they have been updated, are kept in a
+// small save area.
+//
+// Thread layout.  Along x (AXIS 0) a warp holds 32 consecutive cells of one
+// pencil; along y/z a warp holds 32 neighbouring pencils (consecutive x) at
+// the same sweep position.  Both give 256-byte coalesced rows.
+#pragma once
+#include "hp_device.cuh"
+#include "hp_physics.cuh"
+
+namespace hp {
+
+struct SweepArgs {
+    double* f[5];          // p, rho, u (normal), v, w (transverse) of this sweep
+    double* snap[4];       // step-start p, vx, vy, vz (natural order) for expand
+    const double* peak;    // per-face density-peak values for y/z sweeps (may be null)
+    DevCtl* ctl;
+    Consts k;
+    int nx, ny, nz;
+    int nsweep;            // cells along the sweep axis
+    long long npencil;     // pencils in this sweep
+    int bslot;             // rho-bound slot this sweep reads (0..2)
+    int flags;
+};
+
+// Precision policies.  R is the reconstruction/tracing type, Pow the power
+// used by the Riemann solver.
+struct PolicyFP64 {
+    using R = double;
+    using Pow = PowExact;
+};
+
+template <int AXIS>
+__device__ __forceinline__ long long pencil_base(long long pid, int nx, int ny) {
+    if (AXIS == 0) return pid * nx;                                     // (y,z) -> x row
+    if (AXIS == 1) return (pid % nx) + (long long)nx * ny * (pid / nx);  // (x,z)
+    return pid;                                                         // (x,y)
+}
+template <int AXIS>
+__device__ __forceinline__ long long axis_stride(int nx, int ny) {
+    return AXIS == 0 ? 1 : (AXIS == 1 ? (long long)nx : (long long)nx * ny);
+}
+
+template <int AXIS, int P, int T, int RING>
+struct SweepLayout {
+    static constexpr int kThreads = P * T;
+    static constexpr int kCells = P * RING;
+    __device__ __forceinline__ static int idx(int cell, int tp) {
+        const int slot = cell & (RING - 1);
+        return AXIS == 0 ? tp * RING + slot : slot * P + tp;
+    }
+};
+
+template <int AXIS, int P, int T, int RING, class Policy>
+struct SweepSmem {
+    using R = typename Policy::R;
+    double st[5][P * RING];     // state ring: p, rho, u, v, w
+    R sl[5][P * RING];          // ajside slopes
+    R d2[P * RING];             // dda second difference of rho
+    unsigned char pf[P * RING]; // flattening flag of pair (c, c+1)
+    R ls[5][P * RING];          // traced left state (face c+1) from cell c
+    double fs[5][P * RING];     // Riemann face state of face f
+    double sv[5][3 * P];        // original values of cells 0..2
+    unsigned long long red[128];
+};
+
+template <int AXIS, int P, int T, int RING, class Policy>
+__global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
+    using R = typename Policy::R;
+    using Pow = typename Policy::Pow;
+    using L = SweepLayout<AXIS, P, T, RING>;
+    static_assert((RING & (RING - 1)) == 0 && RING >= T + 6, "ring too small");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy>*>(smem_raw);
+
+    const int tid = threadIdx.x;
+    const int tl = AXIS == 0 ? (tid % T) : (tid / P);
+    const int tp = AXIS == 0 ? (tid / T) : (tid % P);
+    const long long pid = (long long)blockIdx.x * P + tp;
+    const bool active = pid < a.npencil;
+    const int N = a.nsweep;
+    const long long base = pencil_base<AXIS>(active ? pid : 0, a.nx, a.ny);
+    const long long stride = axis_stride<AXIS>(a.nx, a.ny);
+
+    const Consts k = a.k;
+    const StepScalars sc = a.ctl->s;
+    const R dt_ = R(sc.dt), rat_ = R(sc.rat), dat_ = R(sc.dat), at_ = R(sc.at);
+    const R dx_ = R(k.dx), gam_ = R(k.gamma), flatv_ = R(k.flatvalue), ming_ = R(k.mingradflat);
+    if (a.ctl->done) return;  // told >= tstop: the time loop has ended (main.F90:200)
+
+    // density-peak fix is possible only if some rho exceeds dmax x another
+    // rho (monotone rounding makes this test exact; see the update epilogue)
+    const double rmin0 = dkey_decode(a.ctl->rho_key[a.bslot][0]);
+    const double rmax0 = dkey_decode(a.ctl->rho_key[a.bslot][1]);
+    const bool peak_possible = rmax0 > k.dmax * rmin0;
+
+    if (tid == 0 && blockIdx.x == 0) {
+        const int reset = (a.bslot + 2) % 3;
+        a.ctl->rho_key[reset][0] = kKeyPosInf;
+        a.ctl->rho_key[reset][1] = kKeyNegInf;
+        if (a.flags & kFlagResetSpeed) a.ctl->velmax_key = 0ULL;
+    }
+
+    // expand.F90:157-159
+    const double afact = sc.dt * (sc.dath / sc.ath);
+    const double afact1 = 1.0 / (1.0 + afact);
+    const double afact2 = 1.0 / (2.0 + afact);
+
+    unsigned long long kmin = kKeyPosInf, kmax = 0ULL, kvel = 0ULL;
+    unsigned status = 0;
+
+    FaceState right;        // right state of face c (cell c), from stage B
+    FaceState face_own;     // Riemann state of face f, from stage C
+
+    for (int b = -4; b <= N + 3; b += T) {
+        const int e = b + tl;
+        __syncthreads();
+        // ---------------- load cell e ----------------
+        if (active && e >= -4 && e <= N + 2) {
+            double v[5];
+            if (e >= N) {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) v[q] = S.sv[q][(e - N) * P + tp];
+            } else {
+                const int s = e < 0 ? e + N : e;
+                const long long g = base + stride * s;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) v[q] = a.f[q][g];
+                if (e >= 0 && e < 3) {
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) S.sv[q][e * P + tp] = v[q];
+                }
+                if ((a.flags & kFlagSnapshot) && e >= 0) {
+                    // natural order p, vx, vy, vz
+                    double vx = AXIS == 0 ? v[2] : (AXIS == 1 ? v[3] : v[4]);
+                    double vy = AXIS == 0 ? v[3] : (AXIS == 1 ? v[2] : v[3]);
+                    double vz = AXIS == 0 ? v[4] : (AXIS == 1 ? v[4] : v[2]);
+                    a.snap[0][g] = v[0];
+                    a.snap[1][g] = vx;
+                    a.snap[2][g] = vy;
+                    a.snap[3][g] = vz;
+                }
+            }
+            const int ix = L::idx(e, tp);
+#pragma unroll
+            for (int q = 0; q < 5; ++q) S.st[q][ix] = v[q];
+        }
+        __syncthreads();
+        // ---------------- A: cell c = e-1 ----------------
+        {
+            const int c = e - 1;
+            if (active && c >= -3 && c <= N + 1) {
+                const int im = L::idx(c - 1, tp), i0 = L::idx(c, tp), ip = L::idx(c + 1, tp);
+                bool flag = false;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const R am = R(S.st[q][im]), a0 = R(S.st[q][i0]), ap = R(S.st[q][ip]);
+                    S.sl[q][i0] = ajside<R>(am, a0, ap);
+                    flag |= flat_pair<R>(a0, ap, ming_);
+                    if (q == 1) S.d2[i0] = dda_second<R>(am, a0, ap, dx_);
+                }
+                S.pf[i0] = flag ? 1 : 0;
+            }
+        }
+        __syncthreads();
+        // ---------------- B: cell c = e-3 ----------------
+        {
+            const int c = e - 3;
+            if (active && c >= -1 && c <= N) {
+                int ic[5];
+#pragma unroll
+                for (int o = 0; o < 5; ++o) ic[o] = L::idx(c - 2 + o, tp);
+                const bool fl_any = S.pf[ic[0]] | S.pf[ic[1]] | S.pf[ic[2]] | S.pf[ic[3]];
+                const R flat = fl_any ? flatv_ : R(0);
+                const R pm1 = R(S.st[0][ic[1]]), p0 = R(S.st[0][ic[2]]), pp1 = R(S.st[0][ic[3]]);
+                const R rm1 = R(S.st[1][ic[1]]), r0 = R(S.st[1][ic[2]]), rp1 = R(S.st[1][ic[3]]);
+                const R addp = fabs(pp1 - pm1) / fmin2(pm1, pp1);
+                const R addrho = R(0.5) * gam_ * fabs(rp1 - rm1) / fmin2(rm1, rp1);
+                const bool steep = addrho >= addp;
+                const R u0 = R(S.st[2][ic[2]]);
+                const R cc = sqrt(gam_ * p0 / r0);
+                // characteristic speeds of the cell (order2interp.F90:194-196,221-223)
+                const R lm = (u0 - cc) * rat_, l0 = u0 * rat_, lp = (u0 + cc) * rat_;
+                // x = y/dx of fl/fr (ppm_functs.F90:59-84); the right-side
+                // arguments are exact negations of the left-side ones.
+                const R yp = dt_ * (u0 + cc) * rat_;
+                const R ym = dt_ * (u0 - cc) * rat_;
+                const R y0 = dt_ * u0 * rat_;
+                const R xp = yp / dx_, xm = ym / dx_, x0 = y0 / dx_;
+                const R xtl = (R(0) > yp) ? R(0) / dx_ : xp;          // max(cv,0), atl
+                const R xtr = (R(0) > -ym) ? R(0) / dx_ : -xm;        // max(cv,0), atr
+                // traced values (t: fl/fr at the face; 1,2,3: the -,0,+ characteristics)
+                R ptl, pc1l = 0, pc2l = 0, pc3l = 0, ptr, pc1r = 0, pc2r = 0, pc3r = 0;
+                R rtl, rc2l = 0, rtr, rc2r = 0;
+                R utl, uc1l = 0, uc3l = 0, utr, uc1r = 0, uc3r = 0;
+                R vtl, vc2l = 0, vtr, vc2r = 0, wtl, wc2l = 0, wtr, wc2r = 0;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) {
+                    const R q1 = R(S.st[q][ic[1]]), q2 = R(S.st[q][ic[2]]), q3 = R(S.st[q][ic[3]]);
+                    const R dm = S.sl[q][ic[1]], d0 = S.sl[q][ic[2]], dp = S.sl[q][ic[3]];
+                    R Dm = 0, Dp = 0;
+                    const bool st = (q == 1) && steep;
+                    if (q == 1) { Dm = S.d2[ic[1]]; Dp = S.d2[ic[3]]; }
+                    const Parabola<R> Pq = build_parabola<R>(q1, q2, q3, dm, d0, dp, flat, st, Dm, Dp, dx_);
+                    const R tl_ = fl(Pq, xtl), tr_ = fr(Pq, xtr);
+                    if (q == 0) {
+                        ptl = tl_; ptr = tr_;
+                        if (lm > R(0)) pc1l = fl(Pq, xm);
+                        if (l0 > R(0)) pc2l = fl(Pq, x0);
+                        if (lp > R(0)) pc3l = fl(Pq, xp);
+                        if (lm < R(0)) pc1r = fr(Pq, -xm);
+                        if (l0 < R(0)) pc2r = fr(Pq, -x0);
+                        if (lp < R(0)) pc3r = fr(Pq, -xp);
+                    } else if (q == 1) {
+                        rtl = tl_; rtr = tr_;
+                        if (l0 > R(0)) rc2l = fl(Pq, x0);
+                        if (l0 < R(0)) rc2r = fr(Pq, -x0);
+                    } else if (q == 2) {
+                        utl = tl_; utr = tr_;
+                        if (lm > R(0)) uc1l = fl(Pq, xm);
+                        if (lp > R(0)) uc3l = fl(Pq, xp);
+                        if (lm < R(0)) uc1r = fr(Pq, -xm);
+                        if (lp < R(0)) uc3r = fr(Pq, -xp);
+                    } else if (q == 3) {
+                        vtl = tl_; vtr = tr_;
+                        if (l0 > R(0)) vc2l = fl(Pq, x0);
+                        if (l0 < R(0)) vc2r = fr(Pq, -x0);
+                    } else {
+                        wtl = tl_; wtr = tr_;
+                        if (l0 > R(0)) wc2l = fl(Pq, x0);
+                        if (l0 < R(0)) wc2r = fr(Pq, -x0);
+                    }
+                }
+                // negative traced states (order2interp.F90:174-190)
+                if (ptl < R(0)) ptl = R(kTiny);
+                if (ptr < R(0)) ptr = R(kTiny);
+                if (rtl < R(0)) rtl = R(kTiny);
+                if (rtr < R(0)) rtr = R(kTiny);
+                const R gz = R(0);  // gravity off: g == 0
+                // left state of face c+1 (order2interp.F90:192-219,249-258)
+                {
+                    const R ctl = sqrt(gam_ * ptl * rtl);
+                    R bml = 0, bpl = 0, b0l = 0, vl = vtl, wl = wtl;
+                    if (lm > R(0)) bml = beta<R>(ctl, utl, uc1l, ptl, pc1l, gz, R(-1), dt_, at_, dat_, rat_);
+                    if (lp > R(0)) bpl = beta<R>(ctl, utl, uc3l, ptl, pc3l, gz, R(1), dt_, at_, dat_, rat_);
+                    if (l0 > R(0)) {
+                        b0l = beta0<R>(ctl, rtl, rc2l, ptl, pc2l, dt_, at_, dat_);
+                        vl = vc2l;
+                        wl = wc2l;
+                    }
+                    R pl = ptl + ctl * ctl * (bpl + bml);
+                    if (pl <= R(0)) pl = ptl;
+                    const R ul = utl + ctl * (bpl - bml);
+                    R rl = R(1) / (R(1) / rtl - bml - b0l - bpl);
+                    if (rl <= R(0)) rl = rtl;
+                    const int io = ic[2];
+                    S.ls[0][io] = pl;
+                    S.ls[1][io] = rl;
+                    S.ls[2][io] = ul;
+                    S.ls[3][io] = vl;
+                    S.ls[4][io] = wl;
+                }
+                // right state of face c (order2interp.F90:221-258)
+                {
+                    const R ctr = sqrt(gam_ * ptr * rtr);
+                    R bpr = 0, bmr = 0, b0r = 0, vr = vtr, wr = wtr;
+                    if (lp < R(0)) bpr = beta<R>(ctr, utr, uc3r, ptr, pc3r, gz, R(1), dt_, at_, dat_, rat_);
+                    if (lm < R(0)) bmr = beta<R>(ctr, utr, uc1r, ptr, pc1r, gz, R(-1), dt_, at_, dat_, rat_);
+                    if (l0 < R(0)) {
+                        b0r = beta0<R>(ctr, rtr, rc2r, ptr, pc2r, dt_, at_, dat_);
+                        vr = vc2r;
+                        wr = wc2r;
+                    }
+                    R pr = ptr + ctr * ctr * (bpr + bmr);
+                    if (pr <= R(0)) pr = ptr;
+                    const R ur = utr + ctr * (bpr - bmr);
+                    R rr = R(1) / (R(1) / rtr - bmr - b0r - bpr);
+                    if (rr <= R(0)) rr = rtr;
+                    right.p = pr;
+                    right.rho = rr;
+                    right.u = ur;
+                    right.v = vr;
+                    right.w = wr;
+                }
+            }
+        }
+        __syncthreads();
+        // ---------------- C: face f = e-3 ----------------
+        {
+            const int f = e - 3;
+            if (active && f >= 0 && f <= N) {
+                const int il = L::idx(f - 1, tp);
+                FaceState left;
+                left.p = double(S.ls[0][il]);
+                left.rho = double(S.ls[1][il]);
+                left.u = double(S.ls[2][il]);
+                left.v = double(S.ls[3][il]);
+                left.w = double(S.ls[4][il]);
+                if (!riemannsolver<Pow>(left, right, face_own, k, sc)) status |= kStatNewton;
+                // density-peak fix (riemannsolver.F90:279-285)
+                if (peak_possible) {
+                    double pk;
+                    if (AXIS == 0) {
+                        pk = peak_value(S.st[1][L::idx(f - 3, tp)], S.st[1][L::idx(f - 2, tp)],
+                                        S.st[1][L::idx(f - 1, tp)], S.st[1][L::idx(f, tp)],
+                                        S.st[2][L::idx(f - 2, tp)], S.st[2][L::idx(f - 1, tp)], k.dmax);
+                    } else {
+                        // the reference gathers these with the x index slot
+                        // (ppmsolver.F90:251-252, 379-380); a pre-pass has
+                        // evaluated them on the pre-sweep state
+                        const int fw = f < N ? f : f - N;
+                        pk = a.peak[base + stride * fw];
+                    }
+                    face_own.p = fmax2(face_own.p, pk);
+                }
+                const int io = L::idx(f, tp);
+                S.fs[0][io] = face_own.p;
+                S.fs[1][io] = face_own.rho;
+                S.fs[2][io] = face_own.u;
+                S.fs[3][io] = face_own.v;
+                S.fs[4][io] = face_own.w;
+            }
+        }
+        __syncthreads();
+        // ---------------- D: cell d = e-4 ----------------
+        {
+            const int d = e - 4;
+            if (active && d >= 0 && d < N) {
+                const int id = L::idx(d, tp);
+                FaceState f1;
+                f1.p = S.fs[0][id];
+                f1.rho = S.fs[1][id];
+                f1.u = S.fs[2][id];
+                f1.v = S.fs[3][id];
+                f1.w = S.fs[4][id];
+                double p = S.st[0][id], rho = S.st[1][id], u = S.st[2][id], v = S.st[3][id], w = S.st[4][id];
+                // total() with the natural component order (ppmsolver.F90:149,277,405)
+                double etot;
+                if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
+                else etot = total_energy(p, rho, u, v, w, k.rgamma1);
+                const double eint = p * k.rgamma1;
+                integrate(f1, face_own, p, rho, u, v, w, etot, eint, k, sc);
+                const long long g = base + stride * d;
+                if (a.flags & kFlagExpand) {
+                    // expand.F90:161-176 with the step-start snapshot
+                    const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
+                    const double vx_o = zero_old ? 0.0 : a.snap[1][g];
+                    const double vy_o = zero_old ? 0.0 : a.snap[2][g];
+                    const double vz_o = zero_old ? 0.0 : a.snap[3][g];
+                    const double p_o = zero_old ? 0.0 : a.snap[0][g];
+                    const double un_o = AXIS == 0 ? vx_o : (AXIS == 1 ? vy_o : vz_o);
+                    const double v_o = AXIS == 0 ? vy_o : (AXIS == 1 ? vx_o : vy_o);
+                    const double w_o = AXIS == 0 ? vz_o : (AXIS == 1 ? vz_o : vx_o);
+                    u = (2.0 * u - afact * un_o) * afact2;
+                    v = (2.0 * v - afact * v_o) * afact2;
+                    w = (2.0 * w - afact * w_o) * afact2;
+                    const double ppp = p;
+                    p = (p - afact * p_o) * afact1;
+                    if (p <= 0.0) p = ppp > 0.0 ? ppp : p_o;
+                }
+                a.f[0][g] = p;
+                a.f[1][g] = rho;
+                a.f[2][g] = u;
+                a.f[3][g] = v;
+                a.f[4][g] = w;
+                const unsigned long long kr = dkey(rho);
+                kmin = kr < kmin ? kr : kmin;
+                kmax = kr > kmax ? kr : kmax;
+                if (a.flags & kFlagSpeed) {
+                    // speed.F90:25-28
+                    const double vs = sqrt(k.gamma * p / rho);
+                    double vm = fabs(u) + vs;
+                    vm = fmax2(vm, fabs(v) + vs);
+                    vm = fmax2(vm, fabs(w) + vs);
+                    const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
+                    kvel = kb > kvel ? kb : kvel;
+                }
+                if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) status |= kStatNaN;
+                else if (rho <= 0.0 || p <= 0.0) status |= kStatNegative;
+            }
+        }
+    }
+    block_flush(kmin, kmax, kvel, status, &a.ctl->rho_key[(a.bslot + 1) % 3][0],
+                &a.ctl->rho_key[(a.bslot + 1) % 3][1], (a.flags & kFlagSpeed) ? &a.ctl->velmax_key : nullptr,
+                &a.ctl->status, S.red);
+}
+
+}  // namespace hp

@@ -1,0 +1,104 @@
+"""Initial conditions for the benchmark configurations.
+
+* :func:`sod` -- the plane-parallel Sod tube (the reference's chooseinit=1/2/3,
+  hydropad/initialize_hydro.F90:35-117) with the interface at x=0.5 and its
+  periodic mirror at x=0.
+* :func:`grf_eds` -- a seeded Gaussian random baryon field on an EdS
+  background with linear-theory velocities and uniform temperature (the
+  cosmological configurations; reference analogue initvel.F90:31-37).
+
+Every function returns ``(p, rho, vx, vy, vz)`` as ghosted Fortran-order
+float64 arrays ``(N+2nb, ...)`` with periodic ghosts filled.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# physical constants of the reference namelists (inputfiles/input.nml)
+BOLTZ = 1.380658e-16
+MH = 1.6605e-24
+MPC_CM = 3.086e24
+
+
+def _ghost(a: np.ndarray, nb: int) -> np.ndarray:
+    out = np.pad(a, nb, mode="wrap")
+    return np.asfortranarray(out)
+
+
+def sod(n, axis: int = 0, nb: int = 3, rho_l=1.0, p_l=1.0, rho_r=0.125, p_r=0.1):
+    """Sod tube along ``axis`` on an ``n`` (int or 3-tuple) periodic grid.
+    Cell centres x=(i+1/2)/N; left state for x<0.5."""
+    shape = (n, n, n) if np.isscalar(n) else tuple(n)
+    N = shape[axis]
+    x = (np.arange(N) + 0.5) / N
+    left = x < 0.5
+    sh = [1, 1, 1]
+    sh[axis] = N
+    rho = np.broadcast_to(np.where(left, rho_l, rho_r).reshape(sh), shape).astype(np.float64)
+    p = np.broadcast_to(np.where(left, p_l, p_r).reshape(sh), shape).astype(np.float64)
+    z = np.zeros(shape)
+    return tuple(_ghost(a, nb) for a in (p, rho, z, z, z))
+
+
+def eds_time(a_start: float):
+    """EdS time variables at a_start as initialize_parameters.F90:133-154
+    sets them (t = a^1.5, H = dat/at)."""
+    f2 = np.float32(2.0) / np.float32(3.0)
+    tin = a_start ** 1.5
+    at = tin ** float(f2)
+    dat = float(f2) * tin ** float(np.float32(-1.0) / np.float32(3.0))
+    return tin, at, dat
+
+
+def temperature_factor(box_mpc_over_h: float = 1.0, hnow: float = 0.7) -> float:
+    """tfact of initialize_parameters.F90:109 (code temperature = T/tfact).
+
+    The code length unit is the box (dx = 1/N, initialize_parameters.F90:23),
+    so xnow is taken as the box length; the reference's line 75 divides it by
+    ngridx, which would make the code temperature depend on the resolution."""
+    box = box_mpc_over_h / hnow
+    xnow = MPC_CM * box
+    h_sec = hnow / 3.0856e17
+    t0h0 = 0.66666666667
+    tnow = t0h0 / h_sec
+    r = BOLTZ / MH
+    return (xnow / tnow) ** 2 / r
+
+
+def grf_eds(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float = 0.5, spectral_index: float = -2.0,
+            kc_frac: float = 1.0 / 8.0, temp_k: float = 100.0, rho_floor: float = 1e-2, nb: int = 3,
+            gamma: float = 5.0 / 3.0):
+    """Gaussian random overdensity with P(k) ~ k^n exp(-(k/kc)^2), k in grid
+    units, kc = kc_frac*N, rms delta normalised to ``rms``; rho = max(1+delta,
+    rho_floor); v_k = i a H f delta_k k/k^2 (f=1, EdS; k in box units);
+    uniform temperature -> p = rho*T/tfact."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    white = rng.standard_normal((n, n, n))
+    wk = np.fft.rfftn(white)
+    kx = np.fft.fftfreq(n) * n
+    kz = np.fft.rfftfreq(n) * n
+    KX, KY, KZ = np.meshgrid(kx, kx, kz, indexing="ij")
+    k2 = KX ** 2 + KY ** 2 + KZ ** 2
+    k = np.sqrt(k2)
+    kc = kc_frac * n
+    with np.errstate(divide="ignore", invalid="ignore"):
+        pk = np.where(k > 0, k ** spectral_index * np.exp(-(k / kc) ** 2), 0.0)
+    dk = wk * np.sqrt(pk)
+    delta = np.fft.irfftn(dk, s=(n, n, n))
+    norm = rms / delta.std()
+    delta *= norm
+    dk *= norm
+    tin, at, dat = eds_time(a_start)
+    hub = dat / at
+    fac = at * hub * 1.0  # a H f
+    two_pi = 2.0 * np.pi
+    with np.errstate(divide="ignore", invalid="ignore"):
+        inv = np.where(k2 > 0, 1.0 / (two_pi * k2), 0.0)  # k_phys/k_phys^2 = k_int/(2 pi k_int^2)
+    vel = []
+    for K in (KX, KY, KZ):
+        vk = 1j * fac * dk * K * inv
+        vel.append(np.fft.irfftn(vk, s=(n, n, n)))
+    rho = np.maximum(1.0 + delta, rho_floor)
+    tcode = temp_k / temperature_factor()
+    p = rho * tcode
+    return tuple(_ghost(np.ascontiguousarray(a), nb) for a in (p, rho, vel[0], vel[1], vel[2]))

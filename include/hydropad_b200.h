@@ -1,0 +1,155 @@
+/*
+ * hydropad_b200.h -- C ABI of the B200 PPM hydro step.
+ *
+ * Drop-in boundary for Hydropad's STENCIL hydro step.  Each entry point names
+ * the reference routine it replaces:
+ *
+ *   hp_ppmsolver   <- SUBROUTINE ppmsolver(p3d,rho3d,vx3d,vy3d,vz3d,cho3d,nes3d,
+ *                                          gforce,nx,ny,nz,nbound,ndirection)
+ *                     hydro/ppmsolver.F90:1-5 (STENCIL argument list)
+ *   hp_ppm_lxlylz  <- SUBROUTINE ppm_lxlylz          hydro/ppm_lxlylz.F90:1-223
+ *                     (+ the exchange_mesh after every sweep,
+ *                      hydropad/exchange_mesh.F90:23-41)
+ *   hp_speed       <- SUBROUTINE speed               hydropad/speed.F90:2-59
+ *   hp_timedet     <- SUBROUTINE timedet / timedet_cosmo
+ *                                                    hydropad/functions.F90:61-210
+ *   hp_evolve      <- the hydro part of SUBROUTINE evolve_sys, nsteps times
+ *                     hydropad/evolve_sys.F90:30-130, main.F90:200-221
+ *   hp_attach_state / hp_sync_to_host
+ *                  <- the `!$acc update device/host` pairs around every sweep
+ *                     (ppmsolver.F90:95, ppm_lxlylz.F90:20), done once per run
+ *   hp_set_scalars <- the `!$acc update device(<module scalar list>)`
+ *                     hydro/ppmsolver.F90:68-69, hydropad/scalar.F90:98-99
+ *
+ * Arrays passed by the caller are the reference's module arrays: REAL(8),
+ * Fortran column-major (nx,ny,nz) INCLUDING nbound ghost layers per side
+ * (hydropad/alloc_arrays.F90:76-78).  The device keeps only the interior,
+ * x fastest, and applies the periodic boundary by index wrap, so the ghost
+ * layers are an output-only convenience (refreshed by hp_sync_to_host).
+ *
+ * All functions return HP_OK (0) or a negative HP_ERR_* code; hp_strerror
+ * names it.  No function is re-entrant on the same context.
+ */
+#ifndef HYDROPAD_B200_H
+#define HYDROPAD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    HP_OK = 0,
+    HP_ERR_ARG = -1,           /* bad argument / shape / unknown direction */
+    HP_ERR_CUDA = -2,          /* a CUDA runtime call failed */
+    HP_ERR_OOM = -3,           /* device allocation failed */
+    HP_ERR_NEWTON = -4,        /* Newton for p* exceeded 100 iterations (riemann.F90:62-65: `stop`) */
+    HP_ERR_NAN = -5,           /* NaN in the updated state */
+    HP_ERR_NEGATIVE_STATE = -6,/* rho <= 0 or p <= 0 in the updated state */
+    HP_ERR_NOT_ATTACHED = -7,  /* sweep requested before hp_attach_state */
+    HP_ERR_STATE_MISMATCH = -8,/* host arrays differ from the attached ones */
+    HP_ERR_NO_DEVICE = -9      /* no CUDA device / wrong architecture */
+};
+
+enum { HP_PREC_FP64 = 0, HP_PREC_MIXED = 1 };
+
+/* Namelist values of the run (hydropad/init_sys.F90:12-44) plus the
+ * precision choice.  ngrid = interior cells per axis of this box. */
+typedef struct {
+    int ngridx, ngridy, ngridz;   /* &MESH ngridx/ngridy/ngridz (interior) */
+    int nbound;                   /* &MESH nbound (ghosts of the HOST arrays) */
+    double gamma;                 /* &PHYSICS gamma */
+    double cour, ca, eta1, eta2, dmax;  /* &NUMERICS */
+    double flatvalue, mingradflat;      /* &PPM */
+    double dtinit, tstop;               /* &TIME */
+    int cosmo;                    /* 1: EdS background (-DCOSMO) */
+    int expand_zero_old;          /* 1: expand with vxold=pold3d=0 (as allocated) */
+    double a_start;               /* initial expansion factor (cosmo) */
+    double dt_cap;                /* timedet_cosmo debug cap dt0; <= 0 disables */
+    int precision;                /* HP_PREC_FP64 or HP_PREC_MIXED */
+    int device;                   /* CUDA device ordinal */
+} hp_params;
+
+/* Time scalars of the module `scalar` read by the step (scalar.F90:17-19). */
+typedef struct {
+    double dt, rdtath, at, dat, rat, ath, dath;
+    double t, told, thalf, dtold, atnew, datnew;
+    double velmax;
+    int nstep;
+    int pad;
+} hp_scalars;
+
+typedef struct hp_ctx hp_ctx;
+
+/* Allocate the device state for one box and initialise the time scalars as
+ * initialize_parameters does (initialize_parameters.F90:133-205). */
+int hp_init(const hp_params *params, hp_ctx **ctx);
+int hp_finalize(hp_ctx *ctx);
+
+int hp_set_scalars(hp_ctx *ctx, const hp_scalars *s);
+int hp_get_scalars(hp_ctx *ctx, hp_scalars *s);
+
+/* Upload the host state (ghosted Fortran arrays) once; it then stays
+ * resident in HBM.  gforce is accepted for ABI compatibility and must be
+ * NULL (gravity off). */
+int hp_attach_state(hp_ctx *ctx, const double *p3d, const double *rho3d,
+                    const double *vx3d, const double *vy3d, const double *vz3d,
+                    const double *gforce, int nx, int ny, int nz, int nbound);
+
+/* Download the resident state into the attached host arrays (interior) and
+ * refill their periodic ghost layers. */
+int hp_sync_to_host(hp_ctx *ctx);
+
+/* Download into arbitrary host arrays of the same shape. */
+int hp_download_state(hp_ctx *ctx, double *p3d, double *rho3d, double *vx3d,
+                      double *vy3d, double *vz3d, int nx, int ny, int nz,
+                      int nbound);
+
+/* Drop-in for ppmsolver: one directional sweep (1=x, 2=y, 3=z) on the
+ * resident state.  The host pointers identify the attached state (they must
+ * be the attached arrays); cho3d/nes3d are unused under STENCIL and may be
+ * NULL.  Scalars and integers are passed by reference, like the Fortran
+ * subroutine.  Returns the sweep's error status. */
+int hp_ppmsolver(hp_ctx *ctx, double *p3d, double *rho3d, double *vx3d,
+                 double *vy3d, double *vz3d, double *cho3d, double *nes3d,
+                 const double *gforce, const int *nx, const int *ny,
+                 const int *nz, const int *nbound, const int *ndirection);
+
+/* Drop-in for ppm_lxlylz: three sweeps in the order nrot selects
+ * (1 xyz, 2 zyx, 3 yzx, 4 xzy, 5 zxy, 6 yxz).  No ghost exchange is needed:
+ * the device state is periodic by construction. */
+int hp_ppm_lxlylz(hp_ctx *ctx, int nrot);
+
+/* speed: velmax = max over cells of max_d(|v_d| + sqrt(gamma p/rho)). */
+int hp_speed(hp_ctx *ctx, double *velmax);
+
+/* timedet (static) or timedet_cosmo (cosmo) on the context's scalars with
+ * the given velmax. */
+int hp_timedet(hp_ctx *ctx, double velmax);
+
+/* nsteps of evolve_sys' hydro part, entirely on the device: nrot schedule,
+ * three fused sweeps, [expand], speed and timedet, no host round trip.
+ * use_graph=1 captures one step per nrot value in CUDA graphs and replays
+ * them.  Returns the accumulated error status. */
+int hp_evolve(hp_ctx *ctx, int nsteps, int use_graph);
+
+/* Block until the context's stream is idle and return the device status
+ * word accumulated since the last call (then cleared). */
+int hp_synchronize(hp_ctx *ctx);
+
+/* CUDA stream the context launches on (cudaStream_t), for event timing. */
+void *hp_stream(hp_ctx *ctx);
+
+/* Device pointers of the resident fields (p, rho, vx, vy, vz), dense
+ * (ngridx,ngridy,ngridz) x fastest, for zero-copy access by the caller. */
+int hp_device_fields(hp_ctx *ctx, double **p, double **rho, double **vx,
+                     double **vy, double **vz);
+
+const char *hp_strerror(int code);
+
+/* Number of kernels launched by this context since creation. */
+long long hp_launch_count(hp_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
