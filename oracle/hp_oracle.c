@@ -619,8 +619,10 @@ int hpo_ppmsolver(double *p3d, double *rho3d, double *vx3d, double *vy3d, double
                         rho[ippm] = rho3d[q];
                         vx[ippm] = (ndirection == 1) ? vx3d[q] : (ndirection == 2) ? vy3d[q] : vz3d[q];
                     } else {
-                        rho[ippm] = 0.0;
-                        vx[ippm] = 0.0;
+                        /* outside the allocation (non-cubic boxes only):
+                         * NaN makes the peak test false */
+                        rho[ippm] = NAN;
+                        vx[ippm] = NAN;
                     }
                 }
                 size_t f = CELL(i, t1, t2);
