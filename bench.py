@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the PPM hydro step (cell-updates/s) -- one JSON line.
+
+Workload: the cosmological box of the headline configuration, 256^3 cells,
+Einstein-de Sitter background from z=50, seeded Gaussian random baryon field
+(rms delta 0.5, P(k) ~ k^-2 exp(-(k/k_c)^2), k_c = N/8), linear velocities,
+T = 100 K.  One step = one evolve_sys hydro step: three fused directional
+sweeps, expand, CFL reduction and timedet, all on the device.  The headline
+value is the mixed-precision path; the FP64 path is measured beside it and
+the density relative L1 between the two is reported.
+
+    python bench.py [--steps K] [--warmup W] [--n 256]
+    torchrun --nproc-per-node N bench.py --gpus N      # one box per GPU (weak)
+    python bench.py --impl reference                   # CPU oracle on host cores
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PPM cell-updates/s, mixed vs FP64 GPU at density rel-L1≤1e-5; p50/p99 latency"
+UNIT = "cell-updates/s"
+BASE_SEED = 12345
+BYTES_PER_CELL_SWEEP = 80  # 5 FP64 fields read + written once per sweep
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(n, world, precision):
+    return {
+        "workload": f"{n}^3 EdS cosmological box (z=50 start, GRF rms 0.5, k_c=N/8, T=100K), one box per GPU",
+        "grid": n,
+        "global_cells": n ** 3 * world,
+        "precision": precision,
+        "ic_seed": f"{BASE_SEED}+rank",
+        "l2_policy": f"state {5 * 8 * n ** 3 / 1e6:.0f} MB per box > 126 MB L2: no flush needed",
+        "parallelism": f"{world} independent boxes (no data-path collective)",
+    }
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        loaded = [v for v in sm if smax and v > 0.5 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from hydropad_b200 import ics
+    from hydropad_b200.api import Hydro
+    from hydropad_b200.params import HydroParams
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n, K, W = args.n, args.steps, args.warmup
+    state = ics.grf_eds(n, seed=BASE_SEED + rank)
+    prm = HydroParams(shape=(n, n, n), cosmo=True, tstop=(1.0 + 10.0) ** (-1.5))
+    cells = float(n) ** 3
+
+    results = {}
+    finals = {}
+    for prec in ("fp64", "mixed"):
+        h = Hydro(prm, precision=prec, device=local)
+        h.attach_state(*state)
+        h.start_with_cfl()
+        h.evolve(W, graph=True)
+        stream = torch.cuda.ExternalStream(h.stream_handle())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = h.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            h.evolve_async(K, graph=True)
+            e1.record(stream)
+            h.synchronize()
+            torch.cuda.synchronize()
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1)) / K
+        results[prec] = {"ms_per_step": ms, "value": world * cells / (ms * 1e-3),
+                         "launches": h.launch_count() - l0, "clocks": clk.summary()}
+        finals[prec] = h.download(nbound=0)
+        # per-sweep duration of the dominant kernel (fused sweep), CUDA events
+        # on the launching stream; 3 sweeps per ppm_lxlylz call
+        reps = 3
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for r in range(reps):
+            h.ppm_lxlylz(1 + r % 6)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        results[prec]["sweep_ms"] = e0.elapsed_time(e1) / (3 * reps)
+        h.close()
+
+    rho64, rhomx = finals["fp64"][1], finals["mixed"][1]
+    dens_l1 = float(np.abs(rhomx - rho64).sum() / np.abs(rho64).sum())
+
+    # end to end through the C ABI with host buffers: upload the ghosted
+    # Fortran arrays from pinned host memory, one step, download + ghost fill
+    e2e = None
+    if not args.no_e2e:
+        nbg = n + 6
+        pinned = [torch.empty(nbg ** 3, dtype=torch.float64, pin_memory=True) for _ in range(5)]
+        host = [p.numpy().reshape((nbg, nbg, nbg), order="F") for p in pinned]
+        for hst, src in zip(host, state):
+            hst[...] = src
+        h = Hydro(prm, precision="mixed", device=local)
+        h.attach_state(*host)
+        h.start_with_cfl()
+        h.evolve(1, graph=True)
+        h.sync_to_host()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(K):
+            h.attach_state(*host)          # H2D of the step's input state
+            h.evolve(1, graph=True)        # the step (status read included)
+            h.sync_to_host()               # D2H of the result + ghost refill
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        barrier()
+        el = max_over_ranks(t1 - t0)
+        moved = 5 * 8 * n ** 3
+        e2e = {"value": world * cells * K / el, "unit": UNIT, "h2d_bytes_per_step": moved,
+               "d2h_bytes_per_step": moved, "ms_per_step": 1e3 * el / K,
+               "path": "hp_attach_state + hp_evolve(1) + hp_sync_to_host, pinned ghosted Fortran arrays"}
+        h.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(state, prm, args)
+
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    mx, fp = results["mixed"], results["fp64"]
+    peaks = load_peaks()
+    sweep_s = mx["sweep_ms"] * 1e-3
+    achieved = BYTES_PER_CELL_SWEEP * cells / sweep_s / 1e9
+    traffic = load_traffic(n)
+    line = {
+        "metric": METRIC,
+        "value": mx["value"],
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": mx["ms_per_step"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 reconstruction + f64 Riemann/update (mixed)",
+        "data": "synthetic (seeded GRF initial conditions)",
+        "config": workload_config(n, world, "mixed"),
+        "fp64": {"value": fp["value"], "ms_per_step": fp["ms_per_step"], "sweep_ms": fp["sweep_ms"],
+                 "roofline_frac": BYTES_PER_CELL_SWEEP * cells / (fp["sweep_ms"] * 1e-3) / 1e9 / peaks[0]},
+        "mixed_over_fp64": mx["value"] / fp["value"],
+        "density_rel_l1_mixed_vs_fp64": dens_l1,
+        "steps_compared": W + K,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks[0], "unit": "GB/s",
+                     "frac": achieved / peaks[0], "traffic": traffic, "peak_source": peaks[1],
+                     "kernel": "ppm_sweep_kernel (mixed)",
+                     "algorithmic_bytes_per_launch": BYTES_PER_CELL_SWEEP * cells},
+        "gpu_launches": mx["launches"],
+        "clocks": mx["clocks"],
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def load_traffic(n):
+    """DRAM bytes per sweep launch from the committed ncu summary (captured
+    on a smaller box and scaled by cells), or None."""
+    path = os.path.join(ROOT, "profiles", "ppm_sweep_traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_cell_sweep:"):
+                    return float(line.split(":")[1]) * n ** 3
+    except OSError:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------------
+# CPU arms (oracle: the reference algorithm restated in C, all host cores)
+# --------------------------------------------------------------------------
+def cpu_baseline(state, prm, args, steps=1):
+    from oracle import hp_oracle
+    from tests.helpers import oracle_first_dt
+
+    threads = args.cpu_threads or os.cpu_count() or 1
+    st = hp_oracle.OracleState(*state)
+    s = hp_oracle.make_scalars(prm)
+    oracle_first_dt(hp_oracle, st, s)
+    t0 = time.perf_counter()
+    st.evolve(s, steps, threads)
+    el = time.perf_counter() - t0
+    n = prm.shape[0]
+    return {"value": steps * float(n) ** 3 / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{steps} full step(s) of the same {n}^3 box, C restatement of the reference "
+                      f"STENCIL path (-O3, OpenMP over pencils, {threads} threads)"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from hydropad_b200 import ics
+    from hydropad_b200.params import HydroParams
+    from oracle import hp_oracle
+    from tests.helpers import oracle_first_dt
+
+    n = args.n
+    threads = args.cpu_threads or os.cpu_count() or 1
+    state = ics.grf_eds(n, seed=BASE_SEED)
+    prm = HydroParams(shape=(n, n, n), cosmo=True, tstop=(1.0 + 10.0) ** (-1.5))
+    st = hp_oracle.OracleState(*state)
+    s = hp_oracle.make_scalars(prm)
+    oracle_first_dt(hp_oracle, st, s)
+    # bounded sample: steps of a 128^3 sub-box of the same recipe keep the
+    # run within minutes on the host cores; the metric is per cell-update
+    sub = min(n, 128)
+    if sub != n:
+        state = ics.grf_eds(sub, seed=BASE_SEED)
+        prm = HydroParams(shape=(sub, sub, sub), cosmo=True, tstop=(1.0 + 10.0) ** (-1.5))
+        st = hp_oracle.OracleState(*state)
+        s = hp_oracle.make_scalars(prm)
+        oracle_first_dt(hp_oracle, st, s)
+    st.evolve(s, args.warmup, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        st.evolve(s, 1, threads)
+        times.append(time.perf_counter() - t0)
+    el = sum(times)
+    val = args.steps * float(sub) ** 3 / el
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded GRF initial conditions)",
+        "config": workload_config(n, 1, "fp64"),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{sub}^3 box of the same recipe, {args.steps} timed steps after {args.warmup} "
+                                   f"warm-up steps; C restatement of the reference STENCIL path, OpenMP "
+                                   f"{threads} threads"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

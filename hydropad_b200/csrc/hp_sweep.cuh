@@ -149,11 +149,16 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
         // ---------------- load cell e ----------------
         if (active && e >= -4 && e <= N + 2) {
             double v[5];
-            if (e >= N) {
+            // Cell e-N (0..2) is overwritten by stage D of the iteration that
+            // holds e' = e-N+4; until then global memory still has the
+            // original value (and the save area may not be written yet when
+            // the pencil is shorter than one iteration).
+            const bool from_save = e >= N && (e + 4) / T > (e - N + 8) / T;
+            if (from_save) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) v[q] = S.sv[q][(e - N) * P + tp];
             } else {
-                const int s = e < 0 ? e + N : e;
+                const int s = e < 0 ? e + N : (e >= N ? e - N : e);
                 const long long g = base + stride * s;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) v[q] = a.f[q][g];
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
 #pragma unroll
                     for (int q = 0; q < 5; ++q) S.sv[q][e * P + tp] = v[q];
                 }
-                if ((a.flags & kFlagSnapshot) && e >= 0) {
+                if ((a.flags & kFlagSnapshot) && e >= 0 && e < N) {
                     // natural order p, vx, vy, vz
                     double vx = AXIS == 0 ? v[2] : (AXIS == 1 ? v[3] : v[4]);
                     double vy = AXIS == 0 ? v[3] : (AXIS == 1 ? v[2] : v[3]);
