@@ -23,7 +23,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
 SOURCES = [
     ("hp_kernels_fp64.cu", ["--fmad=false"]),
-    ("hp_kernels_mixed.cu", []),
+    # FP32 stages may use the hardware approximations (FP64 is unaffected)
+    ("hp_kernels_mixed.cu", ["-use_fast_math"]),
     ("hp_api.cu", []),
 ]
 HEADERS = ["hp_physics.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_launch.h"]

@@ -15,7 +15,7 @@ namespace hp {
 
 struct PolicyMixed {
     using R = float;
-    using Pow = PowExact;
+    using Pow = PowRoot;
 };
 
 constexpr int kPx = 8, kTx = 32, kRingX = 64;

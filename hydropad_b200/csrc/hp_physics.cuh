@@ -35,14 +35,14 @@ struct StepScalars {
 };
 
 // ajside, ppm_functs.F90:167-181: limited slope of the middle cell.
+// Evaluated without a branch (the discarded quotient may be NaN), which keeps
+// the warp converged; the selected value is the reference's.
 template <class R>
 __device__ __forceinline__ R ajside(R am1, R a, R ap1) {
-    if ((ap1 - a) * (a - am1) > R(0)) {
-        R da = R(0.5) * (ap1 - am1);
-        R mn = fmin2(fmin2(fabs(da), R(2) * fabs(a - am1)), R(2) * fabs(ap1 - a));
-        return mn * da / fabs(da);
-    }
-    return R(0);
+    const R da = R(0.5) * (ap1 - am1);
+    const R mn = fmin2(fmin2(fabs(da), R(2) * fabs(a - am1)), R(2) * fabs(ap1 - a));
+    const R v = mn * da / fabs(da);
+    return ((ap1 - a) * (a - am1) > R(0)) ? v : R(0);
 }
 
 // One flattening pair (order2interp.F90:66-71): true when the pair's
@@ -50,11 +50,8 @@ __device__ __forceinline__ R ajside(R am1, R a, R ap1) {
 // assign gradleft in the reference; it contributes nothing new here.
 template <class R>
 __device__ __forceinline__ bool flat_pair(R left, R right, R mingradflat) {
-    if (right * left != R(0)) {
-        R g = fabs((right - left) / fmin2(right, left));
-        return g >= mingradflat;
-    }
-    return false;
+    const R g = fabs((right - left) / fmin2(right, left));
+    return (right * left != R(0)) && (g >= mingradflat);
 }
 
 // Second difference used by dda (dda.F90:198-199), centred on the middle cell.
@@ -147,9 +144,70 @@ __device__ __forceinline__ double rhoshock(double p2, double p1, double rho1, do
     return rho1 * (gamma1 * p2 / p1 + 1.0) / (gamma1 + p2 / p1);
 }
 
-// Power used by the Riemann solver.  PowExact: CUDA pow (the FP64 path).
+// Powers used by the Riemann solver, by exponent: x^m, x^-gf, x^rgamma,
+// x^rm (riemannsolver.F90:63,118-119,126,158,192-199; riemann.F90:360-385).
+//
+// PowExact calls CUDA pow with the run's exponents (the FP64 path).  The
+// call is kept out of line so that the solver's many call sites share one
+// copy of the power routine's code.
+static __device__ __noinline__ double pow_shared(double x, double y) { return pow(x, y); }
+
 struct PowExact {
-    __device__ __forceinline__ static double pw(double x, double y) { return pow(x, y); }
+    __device__ __forceinline__ static double pm(double x, const Consts& k) { return pow_shared(x, k.m); }
+    __device__ __forceinline__ static double pgf(double x, const Consts& k) { return pow_shared(x, -k.gf); }
+    __device__ __forceinline__ static double prg(double x, const Consts& k) { return pow_shared(x, k.rgamma); }
+    __device__ __forceinline__ static double prm(double x, const Consts& k) { return pow_shared(x, k.rm); }
+};
+
+// PowRoot: for gamma with integer n = 1/m (= 2 gamma/(gamma-1); 5 for
+// gamma = 5/3) every exponent is a multiple of 1/n, since gf = 1 - m and
+// rgamma = (2/(gamma-1)) m.  x^(1/n) is seeded in FP32 (hardware log2/exp2)
+// and refined by two Newton steps on y^n = x in FP64, which is accurate to
+// an ulp or two; the other powers follow by products and one division.
+// Falls back to pow() when the exponents are not of that form or x is
+// outside the FP32 seed's range.
+__device__ __forceinline__ double ipow(double y, int n) {
+    double r = y;
+    for (int i = 1; i < n; ++i) r *= y;
+    return r;
+}
+
+static __device__ __noinline__ double root_n(double x, int n) {
+    if (!(x > 1e-30 && x < 1e30)) return pow(x, 1.0 / (double)n);
+    const float xf = (float)x;
+    double y = (double)exp2f(__log2f(xf) * (1.0f / (float)n));
+    const double a = (double)(n - 1) / (double)n, b = 1.0 / (double)n;
+#pragma unroll 1
+    for (int it = 0; it < 2; ++it) y = a * y + b * x / ipow(y, n - 1);
+    return y;
+}
+
+struct PowRoot {
+    // n = 1/m and j = rgamma/m when both are small integers, else 0
+    __device__ __forceinline__ static int nroot(const Consts& k) {
+        const double n = k.rm;
+        return (n == floor(n) && n >= 2.0 && n <= 9.0) ? (int)n : 0;
+    }
+    __device__ __forceinline__ static int jrg(const Consts& k) {
+        const double j = k.rgamma * k.rm;
+        return fabs(j - rint(j)) < 1e-12 && j >= 1.0 && j <= 9.0 ? (int)rint(j) : 0;
+    }
+    __device__ __forceinline__ static double pm(double x, const Consts& k) {
+        const int n = nroot(k);
+        return n ? root_n(x, n) : pow_shared(x, k.m);
+    }
+    __device__ __forceinline__ static double pgf(double x, const Consts& k) {
+        const int n = nroot(k);
+        return n ? root_n(x, n) / x : pow_shared(x, -k.gf);
+    }
+    __device__ __forceinline__ static double prg(double x, const Consts& k) {
+        const int n = nroot(k), j = jrg(k);
+        return (n && j) ? ipow(root_n(x, n), j) : pow_shared(x, k.rgamma);
+    }
+    __device__ __forceinline__ static double prm(double x, const Consts& k) {
+        const int n = nroot(k);
+        return n ? ipow(x, n) : pow_shared(x, k.rm);
+    }
 };
 
 // riemann, riemann.F90:318-400 (van Leer Newton for p*).  Returns false when
@@ -177,19 +235,19 @@ __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, dou
             a = cleft * sqrt(k.gf * pstar / pleft + k.m);
             vprimel = -((a * a + cleft * cleft) / (2.0 * a * a * a));
         } else {
-            const double pw = Pow::pw(rl, k.m);
+            const double pw = Pow::pm(rl, k);
             if ((1.0 - pw) == 0.0) a = cleft * sqrt(k.gf * pstar / pleft + k.m);
             else a = k.m * cleft * (1.0 - pstar / pleft) / (1.0 - pw);
-            vprimel = -((1.0 / cleft) * Pow::pw(rl, -k.gf));
+            vprimel = -((1.0 / cleft) * Pow::pgf(rl, k));
         }
         if (pstar >= pright) {
             b = cright * sqrt(k.gf * pstar / pright + k.m);
             vprimer = (b * b + cright * cright) / (2.0 * b * b * b);
         } else {
-            const double pw = Pow::pw(rr, k.m);
+            const double pw = Pow::pm(rr, k);
             if ((1.0 - pw) == 0.0) b = cright * sqrt(k.gf * pstar / pright + k.m);
             else b = k.m * cright * (1.0 - pstar / pright) / (1.0 - pw);
-            vprimer = (1.0 / cright) * Pow::pw(rr, -k.gf);
+            vprimer = (1.0 / cright) * Pow::pgf(rr, k);
         }
         const double vstarl = vxleft - (pstar - pleft) / a;
         const double vstarr = vxright + (pstar - pright) / b;
@@ -205,13 +263,40 @@ struct FaceState {
     double p, rho, u, v, w;
 };
 
+// Wave pattern riemannsolver will take for these states (riemannsolver.F90:
+// 32-64, 73, 113, 188, 231): 1 two shocks, 2 shock + rarefaction, 3 two
+// rarefactions, 4 vacuum, 5 none (NaN input).  Used only to group problems
+// of one pattern into the same warp; the solver decides again itself.
+template <class Pow>
+__device__ __forceinline__ int riemann_pattern(double pleft, double pright, double rholeft, double rhoright,
+                                               double vxleft, double vxright, const Consts& k) {
+    const double gamma = k.gamma;
+    const double cleft = sqrt(gamma * pleft / rholeft);
+    const double cright = sqrt(gamma * pright / rhoright);
+    double p1, p2, rho1, c1, c2;
+    if (pleft <= pright) {
+        p1 = pleft; p2 = pright; rho1 = rholeft; c1 = cleft; c2 = cright;
+    } else {
+        p1 = pright; p2 = pleft; rho1 = rhoright; c1 = cright; c2 = cleft;
+    }
+    const double dvv = vxleft - vxright;
+    const double dv2s = (p2 - p1) / sqrt(0.5 * rho1 * ((gamma - 1.0) * p1 + (gamma + 1.0) * p2));
+    if (dvv >= dv2s) return 1;
+    const double dv1s = -((2.0 * c2 / (gamma - 1.0)) * (1.0 - Pow::pm(p1 / p2, k)));
+    const double dv2r = -(2.0 * (c1 + c2) * k.rgamma1);
+    if (dvv < dv2s && dvv >= dv1s) return 2;
+    if (dvv < dv1s && dvv > dv2r) return 3;
+    if (dvv <= dv2r) return 4;
+    return 5;
+}
+
 // riemannsolver, riemannsolver.F90:1-285 without the density-peak fix,
 // which the caller applies (it needs neighbouring cells).  Returns false on
 // Newton failure.
 template <class Pow>
 __device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceState& Rt, FaceState& out,
                                               const Consts& k, const StepScalars& s) {
-    const double gamma = k.gamma, m = k.m, rm = k.rm, rgamma = k.rgamma, rgamma1 = k.rgamma1;
+    const double gamma = k.gamma, rgamma1 = k.rgamma1;
     const double pleft = L.p, pright = Rt.p, rholeft = L.rho, rhoright = Rt.rho;
     const double vxleft = L.u, vxright = Rt.u;
     bool ok = true;
@@ -242,16 +327,16 @@ __device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceStat
         else if (vshock1 <= 0.0 && vxm > 0.0) rhom = rhoshock1;
         else { pm = pleft; vxm = vxleft; rhom = rholeft; }
     } else {
-        const double dv1s = -((2.0 * c2 / (gamma - 1.0)) * (1.0 - Pow::pw(p1 / p2, m)));
+        const double dv1s = -((2.0 * c2 / (gamma - 1.0)) * (1.0 - Pow::pm(p1 / p2, k)));
         const double dv2r = -(2.0 * (c1 + c2) * rgamma1);
         if (dvv < dv2s && dvv >= dv1s) {  // shock + rarefaction, :113-184
-            pm = Pow::pw((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
-                             (cleft / Pow::pw(pleft, m) + cright / Pow::pw(pright, m)),
-                         rm);
+            pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
+                              (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
+                          k);
             ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
             if (pleft >= pright) {
                 const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
-                const double rhocont1 = rholeft * Pow::pw(pm / pleft, rgamma);
+                const double rhocont1 = rholeft * Pow::prg(pm / pleft, k);
                 double vshock2;
                 if (rhoshock2 == rhoright) vshock2 = 0.0;
                 else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
@@ -268,7 +353,7 @@ __device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceStat
                 }
             } else {
                 const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
-                const double rhocont2 = rhoright * Pow::pw(pm / pright, rgamma);
+                const double rhocont2 = rhoright * Pow::prg(pm / pright, k);
                 double vshock1;
                 if (rhoshock1 == rholeft) vshock1 = 0.0;
                 else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
@@ -285,13 +370,13 @@ __device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceStat
                 }
             }
         } else if (dvv < dv1s && dvv > dv2r) {  // two rarefactions, :188-227
-            const double zeta = (cright / cleft) * Pow::pw(pleft / pright, m);
+            const double zeta = (cright / cleft) * Pow::pm(pleft / pright, k);
             const double vtleft = vxleft + 2.0 * cleft * rgamma1;
             const double vtright = vxright - 2.0 * cright * rgamma1;
             vxm = (vtleft * zeta + vtright) / (1.0 + zeta);
-            pm = pleft * Pow::pw((gamma - 1.0) * (vtleft - vtright) / (2.0 * cleft * (1.0 + zeta)), rm);
-            const double rhocont1 = rholeft * Pow::pw(pm / pleft, rgamma);
-            const double rhocont2 = rhoright * Pow::pw(pm / pright, rgamma);
+            pm = pleft * Pow::prm((gamma - 1.0) * (vtleft - vtright) / (2.0 * cleft * (1.0 + zeta)), k);
+            const double rhocont1 = rholeft * Pow::prg(pm / pleft, k);
+            const double rhocont2 = rhoright * Pow::prg(pm / pright, k);
             const double vtail2 = vxm + sqrt(gamma * pm / rhocont2);
             const double vhead2 = vxright + cright;
             const double vtail1 = vxm - sqrt(gamma * pm / rhocont1);

@@ -90,7 +90,13 @@ struct SweepSmem {
     R d2[P * RING];             // dda second difference of rho
     unsigned char pf[P * RING]; // flattening flag of pair (c, c+1)
     R ls[5][P * RING];          // traced left state (face c+1) from cell c
-    double fs[5][P * RING];     // Riemann face state of face f
+    // traced right state of face f (from cell f), replaced in place by the
+    // Riemann state of face f: each slot is read and then written by the one
+    // thread that solves that face
+    double rs[5][P * RING];
+    int work[P * T];            // Riemann problems of the iteration, sorted by pattern
+    int cnt[P * T / 32][5];     // per-warp counts of the 5 patterns
+    int nwork;
     double sv[5][3 * P];        // original values of cells 0..2
     unsigned long long red[128];
 };
@@ -141,7 +147,6 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
     unsigned status = 0;
 
     FaceState right;        // right state of face c (cell c), from stage B
-    FaceState face_own;     // Riemann state of face f, from stage C
 
     for (int b = -4; b <= N + 3; b += T) {
         const int e = b + tl;
@@ -225,11 +230,13 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                 const R xp = yp / dx_, xm = ym / dx_, x0 = y0 / dx_;
                 const R xtl = (R(0) > yp) ? R(0) / dx_ : xp;          // max(cv,0), atl
                 const R xtr = (R(0) > -ym) ? R(0) / dx_ : -xm;        // max(cv,0), atr
-                // traced values (t: fl/fr at the face; 1,2,3: the -,0,+ characteristics)
-                R ptl, pc1l = 0, pc2l = 0, pc3l = 0, ptr, pc1r = 0, pc2r = 0, pc3r = 0;
-                R rtl, rc2l = 0, rtr, rc2r = 0;
-                R utl, uc1l = 0, uc3l = 0, utr, uc1r = 0, uc3r = 0;
-                R vtl, vc2l = 0, vtr, vc2r = 0, wtl, wc2l = 0, wtr, wc2r = 0;
+                // traced values (t: fl/fr at the face; 1,2,3: the -,0,+
+                // characteristics).  All are evaluated, branch-free; the
+                // tracing below selects the ones the reference computes.
+                R ptl, pc1l, pc2l, pc3l, ptr, pc1r, pc2r, pc3r;
+                R rtl, rc2l, rtr, rc2r;
+                R utl, uc1l, uc3l, utr, uc1r, uc3r;
+                R vtl, vc2l, vtr, vc2r, wtl, wc2l, wtr, wc2r;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
                     const R q1 = R(S.st[q][ic[1]]), q2 = R(S.st[q][ic[2]]), q3 = R(S.st[q][ic[3]]);
@@ -241,30 +248,21 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                     const R tl_ = fl(Pq, xtl), tr_ = fr(Pq, xtr);
                     if (q == 0) {
                         ptl = tl_; ptr = tr_;
-                        if (lm > R(0)) pc1l = fl(Pq, xm);
-                        if (l0 > R(0)) pc2l = fl(Pq, x0);
-                        if (lp > R(0)) pc3l = fl(Pq, xp);
-                        if (lm < R(0)) pc1r = fr(Pq, -xm);
-                        if (l0 < R(0)) pc2r = fr(Pq, -x0);
-                        if (lp < R(0)) pc3r = fr(Pq, -xp);
+                        pc1l = fl(Pq, xm); pc2l = fl(Pq, x0); pc3l = fl(Pq, xp);
+                        pc1r = fr(Pq, -xm); pc2r = fr(Pq, -x0); pc3r = fr(Pq, -xp);
                     } else if (q == 1) {
                         rtl = tl_; rtr = tr_;
-                        if (l0 > R(0)) rc2l = fl(Pq, x0);
-                        if (l0 < R(0)) rc2r = fr(Pq, -x0);
+                        rc2l = fl(Pq, x0); rc2r = fr(Pq, -x0);
                     } else if (q == 2) {
                         utl = tl_; utr = tr_;
-                        if (lm > R(0)) uc1l = fl(Pq, xm);
-                        if (lp > R(0)) uc3l = fl(Pq, xp);
-                        if (lm < R(0)) uc1r = fr(Pq, -xm);
-                        if (lp < R(0)) uc3r = fr(Pq, -xp);
+                        uc1l = fl(Pq, xm); uc3l = fl(Pq, xp);
+                        uc1r = fr(Pq, -xm); uc3r = fr(Pq, -xp);
                     } else if (q == 3) {
                         vtl = tl_; vtr = tr_;
-                        if (l0 > R(0)) vc2l = fl(Pq, x0);
-                        if (l0 < R(0)) vc2r = fr(Pq, -x0);
+                        vc2l = fl(Pq, x0); vc2r = fr(Pq, -x0);
                     } else {
                         wtl = tl_; wtr = tr_;
-                        if (l0 > R(0)) wc2l = fl(Pq, x0);
-                        if (l0 < R(0)) wc2r = fr(Pq, -x0);
+                        wc2l = fl(Pq, x0); wc2r = fr(Pq, -x0);
                     }
                 }
                 // negative traced states (order2interp.F90:174-190)
@@ -276,14 +274,14 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                 // left state of face c+1 (order2interp.F90:192-219,249-258)
                 {
                     const R ctl = sqrt(gam_ * ptl * rtl);
-                    R bml = 0, bpl = 0, b0l = 0, vl = vtl, wl = wtl;
-                    if (lm > R(0)) bml = beta<R>(ctl, utl, uc1l, ptl, pc1l, gz, R(-1), dt_, at_, dat_, rat_);
-                    if (lp > R(0)) bpl = beta<R>(ctl, utl, uc3l, ptl, pc3l, gz, R(1), dt_, at_, dat_, rat_);
-                    if (l0 > R(0)) {
-                        b0l = beta0<R>(ctl, rtl, rc2l, ptl, pc2l, dt_, at_, dat_);
-                        vl = vc2l;
-                        wl = wc2l;
-                    }
+                    const R bm_ = beta<R>(ctl, utl, uc1l, ptl, pc1l, gz, R(-1), dt_, at_, dat_, rat_);
+                    const R bp_ = beta<R>(ctl, utl, uc3l, ptl, pc3l, gz, R(1), dt_, at_, dat_, rat_);
+                    const R b0_ = beta0<R>(ctl, rtl, rc2l, ptl, pc2l, dt_, at_, dat_);
+                    const R bml = (lm > R(0)) ? bm_ : R(0);
+                    const R bpl = (lp > R(0)) ? bp_ : R(0);
+                    const R b0l = (l0 > R(0)) ? b0_ : R(0);
+                    const R vl = (l0 > R(0)) ? vc2l : vtl;
+                    const R wl = (l0 > R(0)) ? wc2l : wtl;
                     R pl = ptl + ctl * ctl * (bpl + bml);
                     if (pl <= R(0)) pl = ptl;
                     const R ul = utl + ctl * (bpl - bml);
@@ -299,14 +297,14 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                 // right state of face c (order2interp.F90:221-258)
                 {
                     const R ctr = sqrt(gam_ * ptr * rtr);
-                    R bpr = 0, bmr = 0, b0r = 0, vr = vtr, wr = wtr;
-                    if (lp < R(0)) bpr = beta<R>(ctr, utr, uc3r, ptr, pc3r, gz, R(1), dt_, at_, dat_, rat_);
-                    if (lm < R(0)) bmr = beta<R>(ctr, utr, uc1r, ptr, pc1r, gz, R(-1), dt_, at_, dat_, rat_);
-                    if (l0 < R(0)) {
-                        b0r = beta0<R>(ctr, rtr, rc2r, ptr, pc2r, dt_, at_, dat_);
-                        vr = vc2r;
-                        wr = wc2r;
-                    }
+                    const R bp_ = beta<R>(ctr, utr, uc3r, ptr, pc3r, gz, R(1), dt_, at_, dat_, rat_);
+                    const R bm_ = beta<R>(ctr, utr, uc1r, ptr, pc1r, gz, R(-1), dt_, at_, dat_, rat_);
+                    const R b0_ = beta0<R>(ctr, rtr, rc2r, ptr, pc2r, dt_, at_, dat_);
+                    const R bpr = (lp < R(0)) ? bp_ : R(0);
+                    const R bmr = (lm < R(0)) ? bm_ : R(0);
+                    const R b0r = (l0 < R(0)) ? b0_ : R(0);
+                    const R vr = (l0 < R(0)) ? vc2r : vtr;
+                    const R wr = (l0 < R(0)) ? wc2r : wtr;
                     R pr = ptr + ctr * ctr * (bpr + bmr);
                     if (pr <= R(0)) pr = ptr;
                     const R ur = utr + ctr * (bpr - bmr);
@@ -322,60 +320,123 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
         }
         __syncthreads();
         // ---------------- C: face f = e-3 ----------------
+        // The Riemann problems of the iteration are classified by wave
+        // pattern and re-dealt to the threads sorted by pattern, so that a
+        // warp solves problems of one pattern (the patterns take very
+        // different code paths; faces of a smooth flow alternate between
+        // them).  C1 classifies and publishes the right states.
         {
             const int f = e - 3;
+            int mycase = 0;
             if (active && f >= 0 && f <= N) {
-                const int il = L::idx(f - 1, tp);
-                FaceState left;
-                left.p = double(S.ls[0][il]);
-                left.rho = double(S.ls[1][il]);
-                left.u = double(S.ls[2][il]);
-                left.v = double(S.ls[3][il]);
-                left.w = double(S.ls[4][il]);
-                if (!riemannsolver<Pow>(left, right, face_own, k, sc)) status |= kStatNewton;
-                // density-peak fix (riemannsolver.F90:279-285)
-                if (peak_possible) {
-                    double pk;
-                    if (AXIS == 0) {
-                        pk = peak_value(S.st[1][L::idx(f - 3, tp)], S.st[1][L::idx(f - 2, tp)],
-                                        S.st[1][L::idx(f - 1, tp)], S.st[1][L::idx(f, tp)],
-                                        S.st[2][L::idx(f - 2, tp)], S.st[2][L::idx(f - 1, tp)], k.dmax);
-                    } else {
-                        // the reference gathers these with the x index slot
-                        // (ppmsolver.F90:251-252, 379-380); a pre-pass has
-                        // evaluated them on the pre-sweep state
-                        const int fw = f < N ? f : f - N;
-                        pk = a.peak[base + stride * fw];
-                    }
-                    face_own.p = fmax2(face_own.p, pk);
-                }
                 const int io = L::idx(f, tp);
-                S.fs[0][io] = face_own.p;
-                S.fs[1][io] = face_own.rho;
-                S.fs[2][io] = face_own.u;
-                S.fs[3][io] = face_own.v;
-                S.fs[4][io] = face_own.w;
+                S.rs[0][io] = right.p;
+                S.rs[1][io] = right.rho;
+                S.rs[2][io] = right.u;
+                S.rs[3][io] = right.v;
+                S.rs[4][io] = right.w;
+                const int il = L::idx(f - 1, tp);
+                mycase = riemann_pattern<Pow>(double(S.ls[0][il]), right.p, double(S.ls[1][il]), right.rho,
+                                              double(S.ls[2][il]), right.u, k);
             }
+            const int lane = tid & 31, warp = tid >> 5;
+            const unsigned lt = (1u << lane) - 1u;
+            int rank = 0;
+#pragma unroll
+            for (int c4 = 1; c4 <= 5; ++c4) {
+                const unsigned m = __ballot_sync(0xffffffffu, mycase == c4);
+                if (lane == 0) S.cnt[warp][c4 - 1] = __popc(m);
+                if (mycase == c4) rank = __popc(m & lt);
+            }
+            __syncthreads();
+            if (mycase) {
+                int off = 0;
+                for (int c4 = 0; c4 < 5; ++c4) {
+                    int tot = 0, before = 0;
+                    for (int w = 0; w < L::kThreads / 32; ++w) {
+                        tot += S.cnt[w][c4];
+                        before += (w < warp) ? S.cnt[w][c4] : 0;
+                    }
+                    if (c4 + 1 == mycase) {
+                        off += before;
+                        break;
+                    }
+                    off += tot;
+                }
+                S.work[off + rank] = (tp << 16) | f;  // (pencil, face) of the problem
+            }
+            if (tid == 0) {
+                int tot = 0;
+                for (int w = 0; w < L::kThreads / 32; ++w)
+                    for (int c4 = 0; c4 < 5; ++c4) tot += S.cnt[w][c4];
+                S.nwork = tot;
+            }
+        }
+        __syncthreads();
+        // C2: solve problem number tid of the sorted list.
+        if (tid < S.nwork) {
+            const int item = S.work[tid];
+            const int wtp = item >> 16, f = item & 0xffff;
+            const int il = L::idx(f - 1, wtp), io = L::idx(f, wtp);
+            FaceState left, rgt, out;
+            left.p = double(S.ls[0][il]);
+            left.rho = double(S.ls[1][il]);
+            left.u = double(S.ls[2][il]);
+            left.v = double(S.ls[3][il]);
+            left.w = double(S.ls[4][il]);
+            rgt.p = S.rs[0][io];
+            rgt.rho = S.rs[1][io];
+            rgt.u = S.rs[2][io];
+            rgt.v = S.rs[3][io];
+            rgt.w = S.rs[4][io];
+            if (!riemannsolver<Pow>(left, rgt, out, k, sc)) status |= kStatNewton;
+            // density-peak fix (riemannsolver.F90:279-285)
+            if (peak_possible) {
+                double pk;
+                if (AXIS == 0) {
+                    pk = peak_value(S.st[1][L::idx(f - 3, wtp)], S.st[1][L::idx(f - 2, wtp)],
+                                    S.st[1][L::idx(f - 1, wtp)], S.st[1][L::idx(f, wtp)],
+                                    S.st[2][L::idx(f - 2, wtp)], S.st[2][L::idx(f - 1, wtp)], k.dmax);
+                } else {
+                    // the reference gathers these with the x index slot
+                    // (ppmsolver.F90:251-252, 379-380); a pre-pass has
+                    // evaluated them on the pre-sweep state
+                    const long long wbase = pencil_base<AXIS>((long long)blockIdx.x * P + wtp, a.nx, a.ny);
+                    const int fw = f < N ? f : f - N;
+                    pk = a.peak[wbase + stride * fw];
+                }
+                out.p = fmax2(out.p, pk);
+            }
+            S.rs[0][io] = out.p;
+            S.rs[1][io] = out.rho;
+            S.rs[2][io] = out.u;
+            S.rs[3][io] = out.v;
+            S.rs[4][io] = out.w;
         }
         __syncthreads();
         // ---------------- D: cell d = e-4 ----------------
         {
             const int d = e - 4;
             if (active && d >= 0 && d < N) {
-                const int id = L::idx(d, tp);
-                FaceState f1;
-                f1.p = S.fs[0][id];
-                f1.rho = S.fs[1][id];
-                f1.u = S.fs[2][id];
-                f1.v = S.fs[3][id];
-                f1.w = S.fs[4][id];
+                const int id = L::idx(d, tp), id1 = L::idx(d + 1, tp);
+                FaceState f1, f2;
+                f1.p = S.rs[0][id];
+                f1.rho = S.rs[1][id];
+                f1.u = S.rs[2][id];
+                f1.v = S.rs[3][id];
+                f1.w = S.rs[4][id];
+                f2.p = S.rs[0][id1];
+                f2.rho = S.rs[1][id1];
+                f2.u = S.rs[2][id1];
+                f2.v = S.rs[3][id1];
+                f2.w = S.rs[4][id1];
                 double p = S.st[0][id], rho = S.st[1][id], u = S.st[2][id], v = S.st[3][id], w = S.st[4][id];
                 // total() with the natural component order (ppmsolver.F90:149,277,405)
                 double etot;
                 if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
                 else etot = total_energy(p, rho, u, v, w, k.rgamma1);
                 const double eint = p * k.rgamma1;
-                integrate(f1, face_own, p, rho, u, v, w, etot, eint, k, sc);
+                integrate(f1, f2, p, rho, u, v, w, etot, eint, k, sc);
                 const long long g = base + stride * d;
                 if (a.flags & kFlagExpand) {
                     // expand.F90:161-176 with the step-start snapshot

@@ -25,7 +25,7 @@ def emulate(N, T, R):
     FS = {}
     save = {}
     right = {}
-    own = {}
+
 
     def wrap(c):
         return c % N
@@ -75,25 +75,32 @@ def emulate(N, T, R):
                 wr[c % R] = c
                 right[tl] = c
         LS.update(wr)
-        # ---- C ----
+        # ---- C1: publish right states, classify ----
         wr = {}
         for tl, e in enumerate(es):
             f = e - 3
             if 0 <= f <= N:
-                assert LS[(f - 1) % R] == f - 1
                 assert right[tl] == f
-                for x in range(f - 3, f + 1):
-                    state_ok(x)
-                wr[f % R] = f
-                own[tl] = f
+                wr[f % R] = ("right", f)
+        assert len(wr) == len({v for v in wr.values()}), "ring slot collision"
+        FS.update(wr)
+        work = sorted(v[1] for v in wr.values())
+        # ---- C2: any thread solves any face of the iteration ----
+        wr = {}
+        for f in work:
+            assert LS[(f - 1) % R] == f - 1
+            assert FS[f % R] == ("right", f)
+            for x in range(f - 3, f + 1):
+                state_ok(x)
+            wr[f % R] = ("face", f)
         FS.update(wr)
         # ---- D ----
         wr = {}
         for tl, e in enumerate(es):
             d = e - 4
             if 0 <= d < N:
-                assert FS[d % R] == d
-                assert own[tl] == d + 1
+                assert FS[d % R] == ("face", d), (N, T, d, FS[d % R])
+                assert FS[(d + 1) % R] == ("face", d + 1)
                 state_ok(d)
                 wr[d] = ("new", d)
         for d, v in wr.items():
