@@ -49,7 +49,8 @@ class HydroError(RuntimeError):
 EXPORTS = (
     "hp_init", "hp_finalize", "hp_set_scalars", "hp_get_scalars", "hp_attach_state", "hp_sync_to_host",
     "hp_download_state", "hp_ppmsolver", "hp_ppm_lxlylz", "hp_speed", "hp_timedet", "hp_evolve",
-    "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count",
+    "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count", "hp_set_tiles",
+    "hp_get_tiles", "hp_autotune",
 )
 
 _lib = None
@@ -86,6 +87,9 @@ def lib():
     L.hp_strerror.restype = C.c_char_p
     L.hp_launch_count.argtypes = [cp]
     L.hp_launch_count.restype = C.c_longlong
+    L.hp_set_tiles.argtypes = [cp, C.c_int, C.c_int, C.c_int]
+    L.hp_get_tiles.argtypes = [cp, ip]
+    L.hp_autotune.argtypes = [cp, C.c_int]
     for name in EXPORTS:
         if name not in ("hp_stream", "hp_strerror", "hp_launch_count"):
             getattr(L, name).restype = C.c_int

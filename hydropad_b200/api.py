@@ -156,6 +156,20 @@ class Hydro:
     def set_scalars(self, s: L.HpScalars):
         L.check(L.lib().hp_set_scalars(self._ctx, C.byref(s)), "hp_set_scalars")
 
+    # -- launch shape --------------------------------------------------------------
+    def set_tiles(self, tx: int, ty: int, tz: int):
+        L.check(L.lib().hp_set_tiles(self._ctx, int(tx), int(ty), int(tz)), "hp_set_tiles")
+
+    def get_tiles(self):
+        t = (C.c_int * 3)()
+        L.check(L.lib().hp_get_tiles(self._ctx, t), "hp_get_tiles")
+        return tuple(t)
+
+    def autotune(self, reps: int = 2):
+        """Pick the fastest sweep tile per axis on a scratch copy of the state."""
+        L.check(L.lib().hp_autotune(self._ctx, int(reps)), "hp_autotune")
+        return self.get_tiles()
+
     def stream_handle(self) -> int:
         return int(L.lib().hp_stream(self._ctx) or 0)
 

@@ -16,17 +16,12 @@
 #include "hp_launch.h"
 
 namespace hp {
-int launch_sweep_fp64(const Box& b, int axis, int bslot, int flags, cudaStream_t st);
-int launch_sweep_mixed(const Box& b, int axis, int bslot, int flags, cudaStream_t st);
-size_t sweep_smem_bytes_fp64(int axis);
-size_t sweep_smem_bytes_mixed(int axis);
+int launch_sweep_fp64(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st);
+int launch_sweep_mixed(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st);
 
-int launch_sweep(const Box& b, int axis, int bslot, int flags, int precision, cudaStream_t st) {
-    return precision == HP_PREC_MIXED ? launch_sweep_mixed(b, axis, bslot, flags, st)
-                                      : launch_sweep_fp64(b, axis, bslot, flags, st);
-}
-size_t sweep_smem_bytes(int axis, int precision) {
-    return precision == HP_PREC_MIXED ? sweep_smem_bytes_mixed(axis) : sweep_smem_bytes_fp64(axis);
+int launch_sweep(const Box& b, int axis, int tile, int bslot, int flags, int precision, cudaStream_t st) {
+    return precision == HP_PREC_MIXED ? launch_sweep_mixed(b, axis, tile, bslot, flags, st)
+                                      : launch_sweep_fp64(b, axis, tile, bslot, flags, st);
 }
 }  // namespace hp
 
@@ -41,6 +36,7 @@ struct hp_ctx {
     const double* host[5];    // attached host arrays (ghosted, Fortran order)
     int hnx, hny, hnz, hnb;
     bool attached;
+    int tile[3];              // sweep tile shape per axis (hp_set_tiles / hp_autotune)
     cudaGraphExec_t graph[6][3];
     int graph_kernels[6][3];
     long long launches;
@@ -168,7 +164,7 @@ int do_sweep(hp_ctx* x, int axis, int flags) {
     int n = hp::launch_peak_prepass(x->box, axis, bslot, x->stream);
     if (n < 0) return HP_ERR_CUDA;
     x->launches += n;
-    n = hp::launch_sweep(x->box, axis, bslot, flags, x->prm.precision, x->stream);
+    n = hp::launch_sweep(x->box, axis, x->tile[axis], bslot, flags, x->prm.precision, x->stream);
     if (n < 0) return HP_ERR_CUDA;
     x->launches += n;
     x->sweep_count += 1;
@@ -494,6 +490,87 @@ int hp_synchronize(hp_ctx* x) {
 }
 
 void* hp_stream(hp_ctx* x) { return x ? (void*)x->stream : nullptr; }
+
+static void drop_graphs(hp_ctx* x) {
+    for (int r = 0; r < 6; ++r)
+        for (int s = 0; s < 3; ++s)
+            if (x->graph[r][s]) {
+                cudaGraphExecDestroy(x->graph[r][s]);
+                x->graph[r][s] = nullptr;
+            }
+}
+
+int hp_set_tiles(hp_ctx* x, int tile_x, int tile_y, int tile_z) {
+    if (!x) return HP_ERR_ARG;
+    const int t[3] = {tile_x, tile_y, tile_z};
+    for (int a = 0; a < 3; ++a)
+        if (t[a] < 0 || t[a] >= hp::kNumTiles) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    drop_graphs(x);
+    for (int a = 0; a < 3; ++a) x->tile[a] = t[a];
+    return HP_OK;
+}
+
+int hp_get_tiles(hp_ctx* x, int* tiles) {
+    if (!x || !tiles) return HP_ERR_ARG;
+    for (int a = 0; a < 3; ++a) tiles[a] = x->tile[a];
+    return HP_OK;
+}
+
+int hp_autotune(hp_ctx* x, int reps) {
+    if (!x || reps < 1) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    HP_CUDA(cudaSetDevice(x->dev));
+    const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
+    hp::Box sb = x->box;  // scratch copy of the box: the resident state is not touched
+    for (int q = 0; q < 4; ++q) sb.snap[q] = nullptr;
+    int rc = HP_OK;
+    double* fields[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    hp::DevCtl* sctl = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float best[3] = {1e30f, 1e30f, 1e30f};
+    int pick[3] = {x->tile[0], x->tile[1], x->tile[2]};
+    const int bslot = (int)(x->sweep_count % 3);
+    for (int q = 0; q < 5 && rc == HP_OK; ++q) rc = cuda_fail(cudaMalloc(&fields[q], n * sizeof(double)));
+    if (rc == HP_OK) rc = cuda_fail(cudaMalloc(&sctl, sizeof(hp::DevCtl)));
+    if (rc == HP_OK) rc = cuda_fail(cudaEventCreate(&e0));
+    if (rc == HP_OK) rc = cuda_fail(cudaEventCreate(&e1));
+    for (int q = 0; q < 5; ++q) sb.f[q] = fields[q];
+    sb.ctl = sctl;
+    for (int axis = 0; axis < 3 && rc == HP_OK; ++axis) {
+        for (int tile = 0; tile < hp::kNumTiles && rc == HP_OK; ++tile) {
+            for (int q = 0; q < 5 && rc == HP_OK; ++q)
+                rc = cuda_fail(cudaMemcpyAsync(fields[q], x->box.f[q], n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                               x->stream));
+            if (rc == HP_OK)
+                rc = cuda_fail(cudaMemcpyAsync(sctl, x->box.ctl, sizeof(hp::DevCtl), cudaMemcpyDeviceToDevice,
+                                               x->stream));
+            if (rc != HP_OK) break;
+            // warm-up launch, then reps timed launches (each a full sweep)
+            if (hp::launch_sweep(sb, axis, tile, bslot, 0, x->prm.precision, x->stream) < 0) rc = HP_ERR_CUDA;
+            if (rc == HP_OK) rc = cuda_fail(cudaEventRecord(e0, x->stream));
+            for (int r = 0; r < reps && rc == HP_OK; ++r)
+                if (hp::launch_sweep(sb, axis, tile, bslot, 0, x->prm.precision, x->stream) < 0) rc = HP_ERR_CUDA;
+            if (rc == HP_OK) rc = cuda_fail(cudaEventRecord(e1, x->stream));
+            if (rc == HP_OK) rc = cuda_fail(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            if (rc == HP_OK) rc = cuda_fail(cudaEventElapsedTime(&ms, e0, e1));
+            x->launches += reps + 1;
+            if (rc == HP_OK && ms < best[axis]) {
+                best[axis] = ms;
+                pick[axis] = tile;
+            }
+        }
+    }
+    cudaStreamSynchronize(x->stream);
+    for (int q = 0; q < 5; ++q) cudaFree(fields[q]);
+    cudaFree(sctl);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc != HP_OK) return rc;
+    return hp_set_tiles(x, pick[0], pick[1], pick[2]);
+}
 
 int hp_device_fields(hp_ctx* x, double** p, double** rho, double** vx, double** vy, double** vz) {
     if (!x) return HP_ERR_ARG;

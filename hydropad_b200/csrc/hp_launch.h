@@ -18,13 +18,13 @@ struct Box {
 };
 
 // Launches return the number of kernels launched (>= 0) or -1 on a launch error.
-int launch_sweep(const Box& b, int axis, int bslot, int flags, int precision, cudaStream_t st);
+int launch_sweep(const Box& b, int axis, int tile, int bslot, int flags, int precision, cudaStream_t st);
 int launch_peak_prepass(const Box& b, int axis, int bslot, cudaStream_t st);
 int launch_bounds(const Box& b, int slot, cudaStream_t st);
 int launch_speed(const Box& b, cudaStream_t st);
 int launch_timedet(const Box& b, int advance, cudaStream_t st);
 
-// Shared memory a sweep needs (bytes), for the API's capacity checks.
-size_t sweep_smem_bytes(int axis, int precision);
+// Number of tile shapes per axis (hp_sweep_launch.cuh).
+constexpr int kNumTiles = 4;
 
 }  // namespace hp

@@ -132,6 +132,17 @@ int hp_timedet(hp_ctx *ctx, double velmax);
  * them.  Returns the accumulated error status. */
 int hp_evolve(hp_ctx *ctx, int nsteps, int use_graph);
 
+/* Sweep tile shape per axis (0 .. 3; pencils per CTA x cells per window
+ * step).  Results do not depend on the tile, only the speed does.  No
+ * reference counterpart (the reference leaves the launch shape to PGI's
+ * OpenACC compiler, ppmsolver.F90:96 `!num_gangs ... vector_length`). */
+int hp_set_tiles(hp_ctx *ctx, int tile_x, int tile_y, int tile_z);
+int hp_get_tiles(hp_ctx *ctx, int *tiles /* [3] */);
+
+/* Time every tile shape of every axis on a scratch copy of the resident
+ * state (reps sweeps each) and keep the fastest. */
+int hp_autotune(hp_ctx *ctx, int reps);
+
 /* Block until the context's stream is idle and return the device status
  * word accumulated since the last call (then cleared). */
 int hp_synchronize(hp_ctx *ctx);

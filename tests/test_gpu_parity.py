@@ -149,3 +149,36 @@ def test_mixed_close_to_fp64():
             outs.append(h.download())
     e = rel_l1(interior(outs[1][1]), interior(outs[0][1]))
     assert e <= 1e-5, e
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_tiles_bitwise_identical(prec):
+    """Every tile shape computes exactly the same cells (only speed differs)."""
+    n = 24
+    state = grf_state(n, seed=13)
+    prm = params_for((n, n, n), cosmo=True)
+    outs = []
+    for t in range(4):
+        with _hydro(prm, prec) as h:
+            h.attach_state(*state)
+            h.set_tiles(t, t, t)
+            h.start_with_cfl()
+            h.evolve(3, graph=True)
+            outs.append(h.download())
+    for t in range(1, 4):
+        for a, b in zip(outs[0], outs[t]):
+            assert np.array_equal(a, b), t
+
+
+def test_autotune_keeps_state():
+    n = 32
+    state = grf_state(n, seed=17)
+    prm = params_for((n, n, n), cosmo=True)
+    with _hydro(prm, "mixed") as h:
+        h.attach_state(*state)
+        before = h.download()
+        tiles = h.autotune(reps=1)
+        after = h.download()
+    assert all(0 <= t < 4 for t in tiles)
+    for a, b in zip(before, after):
+        assert np.array_equal(a, b)
