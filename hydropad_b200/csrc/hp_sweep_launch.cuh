@@ -13,7 +13,7 @@
 
 namespace hp {
 
-constexpr int kTilesX = 4, kTilesYZ = 4;
+constexpr int kTilesX = 6, kTilesYZ = 6;
 
 template <int AXIS, int P, int T, int RING, class Policy>
 static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
@@ -55,6 +55,8 @@ static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int 
             case 1: return launch_sweep_t<0, 4, 32, 64, Policy>(b, bslot, flags, st);
             case 2: return launch_sweep_t<0, 8, 16, 32, Policy>(b, bslot, flags, st);
             case 3: return launch_sweep_t<0, 4, 16, 32, Policy>(b, bslot, flags, st);
+            case 4: return launch_sweep_t<0, 16, 32, 64, Policy>(b, bslot, flags, st);
+            case 5: return launch_sweep_t<0, 12, 32, 64, Policy>(b, bslot, flags, st);
         }
     } else if (axis == 1) {
         switch (tile) {
@@ -62,6 +64,8 @@ static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int 
             case 1: return launch_sweep_t<1, 16, 8, 16, Policy>(b, bslot, flags, st);
             case 2: return launch_sweep_t<1, 32, 4, 16, Policy>(b, bslot, flags, st);
             case 3: return launch_sweep_t<1, 16, 4, 16, Policy>(b, bslot, flags, st);
+            case 4: return launch_sweep_t<1, 64, 8, 16, Policy>(b, bslot, flags, st);
+            case 5: return launch_sweep_t<1, 32, 12, 32, Policy>(b, bslot, flags, st);
         }
     } else if (axis == 2) {
         switch (tile) {
@@ -69,6 +73,8 @@ static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int 
             case 1: return launch_sweep_t<2, 16, 8, 16, Policy>(b, bslot, flags, st);
             case 2: return launch_sweep_t<2, 32, 4, 16, Policy>(b, bslot, flags, st);
             case 3: return launch_sweep_t<2, 16, 4, 16, Policy>(b, bslot, flags, st);
+            case 4: return launch_sweep_t<2, 64, 8, 16, Policy>(b, bslot, flags, st);
+            case 5: return launch_sweep_t<2, 32, 12, 32, Policy>(b, bslot, flags, st);
         }
     }
     return -1;
