@@ -27,7 +27,8 @@ SOURCES = [
     ("hp_kernels_mixed.cu", ["-use_fast_math"]),
     ("hp_api.cu", []),
 ]
-HEADERS = ["hp_physics.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_sweep_launch.cuh", "hp_launch.h"]
+HEADERS = ["hp_physics.cuh", "hp_riemann.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_sweep_launch.cuh",
+           "hp_launch.h"]
 
 
 def _nvcc() -> str:

@@ -272,6 +272,16 @@ int hp_init(const hp_params* p, hp_ctx** out) {
     k.dmax = p->dmax;
     k.eta1 = p->eta1;
     k.eta2 = p->eta2;
+    // exponents of the Riemann solver as multiples of 1/n (see PowRoot)
+    k.nroot = 0;
+    k.jrg = 0;
+    {
+        const double n = k.rm, j = k.rgamma * k.rm;
+        if (n == floor(n) && n >= 2.0 && n <= 9.0) {
+            k.nroot = (int)n;
+            if (fabs(j - rint(j)) < 1e-12 && j >= 1.0 && j <= 9.0) k.jrg = (int)rint(j);
+        }
+    }
 
     hp::DevCtl& c = *x->ctl_pinned;
     memset(&c, 0, sizeof c);

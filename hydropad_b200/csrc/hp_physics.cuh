@@ -29,6 +29,8 @@ template <class R> __device__ __forceinline__ R fmax2(R a, R b) { return b > a ?
 struct Consts {
     double gamma, rgamma, gamma1, rgamma1, m, rm, gf;
     double mingradflat, flatvalue, dmax, eta1, eta2, dx, rdx;
+    int nroot;  // 1/m when it is an integer in [2, 9] (5 for gamma = 5/3), else 0
+    int jrg;    // rgamma/m when nroot != 0 and it is an integer in [1, 9], else 0
 };
 struct StepScalars {
     double dt, rdtath, at, dat, rat, ath, dath;
@@ -134,294 +136,9 @@ __device__ __forceinline__ R beta0(R ct, R rhot, R rhoc, R pt, R pc, R dt, R at,
     return (pt - pc) / (ct * ct) + R(1) / rhot - R(1) / rhoc + (R(2) * dat * pc) / (at * ct * ct) * dt;
 }
 
-// ------------------------------------------------------------------------
-// Riemann solver (FP64 always).  hydro/riemannsolver.F90
-// ------------------------------------------------------------------------
-__device__ __forceinline__ double rarwave(double f1, double f2, double vt, double vh) {  // :290-298
-    return f2 + vt * (f1 - f2) / (vt - vh);
-}
-__device__ __forceinline__ double rhoshock(double p2, double p1, double rho1, double gamma1) {  // :303-313
-    return rho1 * (gamma1 * p2 / p1 + 1.0) / (gamma1 + p2 / p1);
-}
-
-// Powers used by the Riemann solver, by exponent: x^m, x^-gf, x^rgamma,
-// x^rm (riemannsolver.F90:63,118-119,126,158,192-199; riemann.F90:360-385).
-//
-// PowExact calls CUDA pow with the run's exponents (the FP64 path).  The
-// call is kept out of line so that the solver's many call sites share one
-// copy of the power routine's code.
-static __device__ __noinline__ double pow_shared(double x, double y) { return pow(x, y); }
-
-struct PowExact {
-    __device__ __forceinline__ static double pm(double x, const Consts& k) { return pow_shared(x, k.m); }
-    __device__ __forceinline__ static double pgf(double x, const Consts& k) { return pow_shared(x, -k.gf); }
-    __device__ __forceinline__ static double prg(double x, const Consts& k) { return pow_shared(x, k.rgamma); }
-    __device__ __forceinline__ static double prm(double x, const Consts& k) { return pow_shared(x, k.rm); }
-};
-
-// PowRoot: for gamma with integer n = 1/m (= 2 gamma/(gamma-1); 5 for
-// gamma = 5/3) every exponent is a multiple of 1/n, since gf = 1 - m and
-// rgamma = (2/(gamma-1)) m.  x^(1/n) is seeded in FP32 (hardware log2/exp2)
-// and refined by two Newton steps on y^n = x in FP64, which is accurate to
-// an ulp or two; the other powers follow by products and one division.
-// Falls back to pow() when the exponents are not of that form or x is
-// outside the FP32 seed's range.
-__device__ __forceinline__ double ipow(double y, int n) {
-    double r = y;
-    for (int i = 1; i < n; ++i) r *= y;
-    return r;
-}
-
-static __device__ __noinline__ double root_n(double x, int n) {
-    if (!(x > 1e-30 && x < 1e30)) return pow(x, 1.0 / (double)n);
-    const float xf = (float)x;
-    double y = (double)exp2f(__log2f(xf) * (1.0f / (float)n));
-    const double a = (double)(n - 1) / (double)n, b = 1.0 / (double)n;
-#pragma unroll 1
-    for (int it = 0; it < 2; ++it) y = a * y + b * x / ipow(y, n - 1);
-    return y;
-}
-
-struct PowRoot {
-    // n = 1/m and j = rgamma/m when both are small integers, else 0
-    __device__ __forceinline__ static int nroot(const Consts& k) {
-        const double n = k.rm;
-        return (n == floor(n) && n >= 2.0 && n <= 9.0) ? (int)n : 0;
-    }
-    __device__ __forceinline__ static int jrg(const Consts& k) {
-        const double j = k.rgamma * k.rm;
-        return fabs(j - rint(j)) < 1e-12 && j >= 1.0 && j <= 9.0 ? (int)rint(j) : 0;
-    }
-    __device__ __forceinline__ static double pm(double x, const Consts& k) {
-        const int n = nroot(k);
-        return n ? root_n(x, n) : pow_shared(x, k.m);
-    }
-    __device__ __forceinline__ static double pgf(double x, const Consts& k) {
-        const int n = nroot(k);
-        return n ? root_n(x, n) / x : pow_shared(x, -k.gf);
-    }
-    __device__ __forceinline__ static double prg(double x, const Consts& k) {
-        const int n = nroot(k), j = jrg(k);
-        return (n && j) ? ipow(root_n(x, n), j) : pow_shared(x, k.rgamma);
-    }
-    __device__ __forceinline__ static double prm(double x, const Consts& k) {
-        const int n = nroot(k);
-        return n ? ipow(x, n) : pow_shared(x, k.rm);
-    }
-};
-
-// riemann, riemann.F90:318-400 (van Leer Newton for p*).  Returns false when
-// more than 100 iterations would be needed (the reference stops the run).
-template <class Pow>
-__device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, double pleft, double pright,
-                                               double rholeft, double rhoright, double vxleft, double vxright,
-                                               const Consts& k) {
-    double err = 1.e10;
-    int nnewt = 0;
-    const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
-    const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft + vxright);
-    if (pcheck > 0.0) pstar = pcheck;
-    const double cleft = sqrt(k.gamma * pleft * rholeft);
-    const double cright = sqrt(k.gamma * pright * rhoright);
-    while (err > kTerr) {
-        nnewt = nnewt + 1;
-        if (nnewt > kNewtonMax) return false;
-        const double pstarold = pstar;
-        double a, b, vprimel, vprimer;
-        // pstup (:360,:368) is only consulted on the rarefaction side, so the
-        // power is evaluated there alone.
-        const double rl = pstar / pleft, rr = pstar / pright;
-        if (pstar >= pleft) {
-            a = cleft * sqrt(k.gf * pstar / pleft + k.m);
-            vprimel = -((a * a + cleft * cleft) / (2.0 * a * a * a));
-        } else {
-            const double pw = Pow::pm(rl, k);
-            if ((1.0 - pw) == 0.0) a = cleft * sqrt(k.gf * pstar / pleft + k.m);
-            else a = k.m * cleft * (1.0 - pstar / pleft) / (1.0 - pw);
-            vprimel = -((1.0 / cleft) * Pow::pgf(rl, k));
-        }
-        if (pstar >= pright) {
-            b = cright * sqrt(k.gf * pstar / pright + k.m);
-            vprimer = (b * b + cright * cright) / (2.0 * b * b * b);
-        } else {
-            const double pw = Pow::pm(rr, k);
-            if ((1.0 - pw) == 0.0) b = cright * sqrt(k.gf * pstar / pright + k.m);
-            else b = k.m * cright * (1.0 - pstar / pright) / (1.0 - pw);
-            vprimer = (1.0 / cright) * Pow::pgf(rr, k);
-        }
-        const double vstarl = vxleft - (pstar - pleft) / a;
-        const double vstarr = vxright + (pstar - pright) / b;
-        pstar = pstar - (vstarl - vstarr) / (vprimel - vprimer);
-        if (pstar <= 0.0) pstar = pstarold / 1000.0;
-        vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
-        err = fabs(pstarold - pstar) / pstarold;
-    }
-    return true;
-}
-
 struct FaceState {
     double p, rho, u, v, w;
 };
-
-// Wave pattern riemannsolver will take for these states (riemannsolver.F90:
-// 32-64, 73, 113, 188, 231): 1 two shocks, 2 shock + rarefaction, 3 two
-// rarefactions, 4 vacuum, 5 none (NaN input).  Used only to group problems
-// of one pattern into the same warp; the solver decides again itself.
-template <class Pow>
-__device__ __forceinline__ int riemann_pattern(double pleft, double pright, double rholeft, double rhoright,
-                                               double vxleft, double vxright, const Consts& k) {
-    const double gamma = k.gamma;
-    const double cleft = sqrt(gamma * pleft / rholeft);
-    const double cright = sqrt(gamma * pright / rhoright);
-    double p1, p2, rho1, c1, c2;
-    if (pleft <= pright) {
-        p1 = pleft; p2 = pright; rho1 = rholeft; c1 = cleft; c2 = cright;
-    } else {
-        p1 = pright; p2 = pleft; rho1 = rhoright; c1 = cright; c2 = cleft;
-    }
-    const double dvv = vxleft - vxright;
-    const double dv2s = (p2 - p1) / sqrt(0.5 * rho1 * ((gamma - 1.0) * p1 + (gamma + 1.0) * p2));
-    if (dvv >= dv2s) return 1;
-    const double dv1s = -((2.0 * c2 / (gamma - 1.0)) * (1.0 - Pow::pm(p1 / p2, k)));
-    const double dv2r = -(2.0 * (c1 + c2) * k.rgamma1);
-    if (dvv < dv2s && dvv >= dv1s) return 2;
-    if (dvv < dv1s && dvv > dv2r) return 3;
-    if (dvv <= dv2r) return 4;
-    return 5;
-}
-
-// riemannsolver, riemannsolver.F90:1-285 without the density-peak fix,
-// which the caller applies (it needs neighbouring cells).  Returns false on
-// Newton failure.
-template <class Pow>
-__device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceState& Rt, FaceState& out,
-                                              const Consts& k, const StepScalars& s) {
-    const double gamma = k.gamma, rgamma1 = k.rgamma1;
-    const double pleft = L.p, pright = Rt.p, rholeft = L.rho, rhoright = Rt.rho;
-    const double vxleft = L.u, vxright = Rt.u;
-    bool ok = true;
-    const double cleft = sqrt(gamma * pleft / rholeft);
-    const double cright = sqrt(gamma * pright / rhoright);
-    const double dadt = 1.0 - 0.5 * s.dat * s.dt * s.rat;
-    double p1, p2, rho1, c1, c2;
-    if (pleft <= pright) {
-        p1 = pleft; p2 = pright; rho1 = rholeft; c1 = cleft; c2 = cright;
-    } else {
-        p1 = pright; p2 = pleft; rho1 = rhoright; c1 = cright; c2 = cleft;
-    }
-    const double dvv = vxleft - vxright;
-    const double dv2s = (p2 - p1) / sqrt(0.5 * rho1 * ((gamma - 1.0) * p1 + (gamma + 1.0) * p2));
-    double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
-    if (dvv >= dv2s) {  // two shocks, :73-109
-        pm = fmax2(pleft, pright);
-        ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
-        const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
-        const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
-        double vshock1, vshock2;
-        if (rhoshock1 == rholeft) vshock1 = 0.0;
-        else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
-        if (rhoshock2 == rhoright) vshock2 = 0.0;
-        else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
-        if (vshock2 < 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-        else if (vxm <= 0.0 && vshock2 >= 0.0) rhom = rhoshock2;
-        else if (vshock1 <= 0.0 && vxm > 0.0) rhom = rhoshock1;
-        else { pm = pleft; vxm = vxleft; rhom = rholeft; }
-    } else {
-        const double dv1s = -((2.0 * c2 / (gamma - 1.0)) * (1.0 - Pow::pm(p1 / p2, k)));
-        const double dv2r = -(2.0 * (c1 + c2) * rgamma1);
-        if (dvv < dv2s && dvv >= dv1s) {  // shock + rarefaction, :113-184
-            pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
-                              (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
-                          k);
-            ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
-            if (pleft >= pright) {
-                const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
-                const double rhocont1 = rholeft * Pow::prg(pm / pleft, k);
-                double vshock2;
-                if (rhoshock2 == rhoright) vshock2 = 0.0;
-                else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
-                const double vtail1 = vxm - sqrt(gamma * pm / rhocont1);
-                const double vhead1 = vxleft - cleft;
-                if (vshock2 < 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-                else if (vhead1 >= 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-                else if (vxm <= 0.0 && vshock2 >= 0.0) rhom = rhoshock2;
-                else if (vxm > 0.0 && vtail1 <= 0.0) rhom = rhocont1;
-                else if (vtail1 > 0.0 && vhead1 <= 0.0) {
-                    pm = rarwave(pleft, pm, vtail1, vhead1);
-                    rhom = rarwave(rholeft, rhocont1, vtail1, vhead1);
-                    vxm = rarwave(vxleft, vxm, vtail1, vhead1);
-                }
-            } else {
-                const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
-                const double rhocont2 = rhoright * Pow::prg(pm / pright, k);
-                double vshock1;
-                if (rhoshock1 == rholeft) vshock1 = 0.0;
-                else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
-                const double vtail2 = vxm + sqrt(gamma * pm / rhocont2);
-                const double vhead2 = vxright + cright;
-                if (vshock1 > 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-                else if (vhead2 <= 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-                else if (vxm >= 0.0 && vshock1 <= 0.0) rhom = rhoshock1;
-                else if (vxm < 0.0 && vtail2 >= 0.0) rhom = rhocont2;
-                else if (vtail2 < 0.0 && vhead2 >= 0.0) {
-                    pm = rarwave(pright, pm, vtail2, vhead2);
-                    rhom = rarwave(rhoright, rhocont2, vtail2, vhead2);
-                    vxm = rarwave(vxright, vxm, vtail2, vhead2);
-                }
-            }
-        } else if (dvv < dv1s && dvv > dv2r) {  // two rarefactions, :188-227
-            const double zeta = (cright / cleft) * Pow::pm(pleft / pright, k);
-            const double vtleft = vxleft + 2.0 * cleft * rgamma1;
-            const double vtright = vxright - 2.0 * cright * rgamma1;
-            vxm = (vtleft * zeta + vtright) / (1.0 + zeta);
-            pm = pleft * Pow::prm((gamma - 1.0) * (vtleft - vtright) / (2.0 * cleft * (1.0 + zeta)), k);
-            const double rhocont1 = rholeft * Pow::prg(pm / pleft, k);
-            const double rhocont2 = rhoright * Pow::prg(pm / pright, k);
-            const double vtail2 = vxm + sqrt(gamma * pm / rhocont2);
-            const double vhead2 = vxright + cright;
-            const double vtail1 = vxm - sqrt(gamma * pm / rhocont1);
-            const double vhead1 = vxleft - cleft;
-            if (vhead2 <= 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-            else if (vhead1 >= 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-            else if (vhead2 > 0.0 && vtail2 <= 0.0) {
-                pm = rarwave(pright, pm, vtail2, vhead2);
-                rhom = rarwave(rhoright, rhocont2, vtail2, vhead2);
-                vxm = rarwave(vxright, vxm, vtail2, vhead2);
-            } else if (vxm <= 0.0 && vtail2 > 0.0) rhom = rhocont2;
-            else if (vxm > 0.0 && vtail1 <= 0.0) rhom = rhocont1;
-            else if (vtail1 > 0.0 && vhead1 <= 0.0) {
-                pm = rarwave(pleft, pm, vtail1, vhead1);
-                rhom = rarwave(rholeft, rhocont1, vtail1, vhead1);
-                vxm = rarwave(vxleft, vxm, vtail1, vhead1);
-            }
-        } else if (dvv <= dv2r) {  // vacuum, :231-264
-            pm = 0.0; vxm = 0.0;
-            const double rhocont1 = 0.0, rhocont2 = 0.0;
-            const double vtail2 = vxright - 2.0 * cright * rgamma1;
-            const double vhead2 = vxright + cright;
-            const double vtail1 = vxleft - 2.0 * cleft * rgamma1;
-            const double vhead1 = vxleft - cleft;
-            if (vhead2 <= 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-            else if (vhead1 >= 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-            else if (vhead2 > 0.0 && vtail2 <= 0.0) {
-                pm = rarwave(pright, pm, vtail2, vhead2);
-                rhom = rarwave(rhoright, rhocont2, vtail2, vhead2);
-                vxm = rarwave(vxright, vxm, vtail2, vhead2);
-            } else if (vtail1 <= 0.0 && vtail2 > 0.0) rhom = 0.0;
-            else if (vtail1 > 0.0 && vhead1 <= 0.0) {
-                pm = rarwave(pleft, pm, vtail1, vhead1);
-                rhom = rarwave(rholeft, rhocont1, vtail1, vhead1);
-                vxm = rarwave(vxleft, vxm, vtail1, vhead1);
-            }
-        }
-    }
-    // transverse upwinding, :269-275
-    double vym, vzm;
-    if (vxm >= 0.0) { vym = dadt * L.v; vzm = dadt * L.w; }
-    else { vym = dadt * Rt.v; vzm = dadt * Rt.w; }
-    out.p = pm; out.rho = rhom; out.u = vxm; out.v = vym; out.w = vzm;
-    return ok;
-}
 
 // Density-peak pressure fix, riemannsolver.F90:279-285.  r1..r4 / u2,u3 are
 // rhobar(1..4) / vxbar(2..3) of the gather (cells f-3..f of the sweep).

@@ -1,0 +1,373 @@
+// hp_riemann.cuh -- exact Riemann solver of the PPM step, split by wave
+// pattern (hydro/riemannsolver.F90, hydro/riemann.F90).
+//
+// riemannsolver.F90 first classifies the face into one of four wave
+// patterns (:61-64,73,113,188,231) and then runs very different code for
+// each.  The sweep kernel classifies all faces of a window step, groups the
+// faces of one pattern into the same warps, and calls the pattern's solver
+// below; riemannsolver() chains the same pieces for a single face.  Every
+// branch keeps the reference's operand order, so the FP64 instantiation
+// follows the Fortran arithmetic.
+#pragma once
+#include "hp_physics.cuh"
+
+namespace hp {
+
+__device__ __forceinline__ double rarwave(double f1, double f2, double vt, double vh) {  // :290-298
+    return f2 + vt * (f1 - f2) / (vt - vh);
+}
+__device__ __forceinline__ double rhoshock(double p2, double p1, double rho1, double gamma1) {  // :303-313
+    return rho1 * (gamma1 * p2 / p1 + 1.0) / (gamma1 + p2 / p1);
+}
+
+// ------------------------------------------------------------------------
+// Powers by exponent: x^m, x^-gf, x^rgamma, x^rm
+// (riemannsolver.F90:63,118-119,126,158,192-199; riemann.F90:360-385).
+// ------------------------------------------------------------------------
+
+// CUDA pow, out of line so that all call sites share one copy of its code.
+static __device__ __noinline__ double pow_shared(double x, double y) { return pow(x, y); }
+
+// x^(1/n) for integer n >= 2: an FP32 estimate (hardware log2/exp2) refined
+// by two Newton steps on y^n = x in FP64.  The FP32 estimate is good to
+// ~2^-22, so two quadratic steps reach the FP64 rounding level.  Inputs
+// outside the FP32 range go to pow().
+template <int N>
+__device__ __forceinline__ double root_fixed(double x) {
+    if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, 1.0 / (double)N);
+    double y = (double)exp2f(__log2f((float)x) * (1.0f / (float)N));
+    constexpr double a = (double)(N - 1) / (double)N, b = 1.0 / (double)N;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {
+        double yn1 = y;
+#pragma unroll
+        for (int i = 2; i < N; ++i) yn1 *= y;
+        y = a * y + b * x / yn1;
+    }
+    return y;
+}
+
+static __device__ __noinline__ double root_any(double x, int n) {
+    if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, 1.0 / (double)n);
+    double y = (double)exp2f(__log2f((float)x) * (1.0f / (float)n));
+    const double a = (double)(n - 1) / (double)n, b = 1.0 / (double)n;
+#pragma unroll 1
+    for (int it = 0; it < 2; ++it) {
+        double yn1 = y;
+        for (int i = 2; i < n; ++i) yn1 *= y;
+        y = a * y + b * x / yn1;
+    }
+    return y;
+}
+
+__device__ __forceinline__ double ipow(double y, int n) {
+    double r = y;
+    for (int i = 1; i < n; ++i) r *= y;
+    return r;
+}
+
+// gamma enters the Riemann solver only through m = (gamma-1)/(2 gamma),
+// gf = 1 - m, rgamma and rm = 1/m.  When n = 1/m is an integer (5 for
+// gamma = 5/3; k.nroot) and rgamma = j m with integer j (3 for 5/3; k.jrg),
+// every power is a product of x^(1/n) and x: x^m = r, x^-gf = r/x,
+// x^rgamma = r^j, x^rm = x^n.  These agree with pow() to an ulp or two.
+// Other gammas use pow().
+struct PowRoot {
+    __device__ __forceinline__ static double root(double x, const Consts& k) {
+        return k.nroot == 5 ? root_fixed<5>(x) : root_any(x, k.nroot);
+    }
+    __device__ __forceinline__ static double pm(double x, const Consts& k) {
+        return k.nroot ? root(x, k) : pow_shared(x, k.m);
+    }
+    __device__ __forceinline__ static double pgf(double x, const Consts& k) {
+        return k.nroot ? root(x, k) / x : pow_shared(x, -k.gf);
+    }
+    __device__ __forceinline__ static double prg(double x, const Consts& k) {
+        return (k.nroot && k.jrg) ? ipow(root(x, k), k.jrg) : pow_shared(x, k.rgamma);
+    }
+    __device__ __forceinline__ static double prm(double x, const Consts& k) {
+        return k.nroot ? ipow(x, k.nroot) : pow_shared(x, k.rm);
+    }
+};
+
+// FP32 powers for the mixed path's closed-form two-rarefaction solution.
+struct PowF32 {
+    __device__ __forceinline__ static float pw(float x, float y) { return exp2f(y * __log2f(x)); }
+};
+
+// ------------------------------------------------------------------------
+// Classification, riemannsolver.F90:32-64 + the tests at :73,113,188,231.
+// Returns 1 two shocks, 2 shock + rarefaction, 3 two rarefactions,
+// 4 vacuum, 5 none (NaN input).  cleft/cright are reused by the solvers.
+// ------------------------------------------------------------------------
+template <class T, class PowT>
+__device__ __forceinline__ int riemann_classify(T pleft, T pright, T rholeft, T rhoright, T vxleft, T vxright,
+                                                T& cleft, T& cright, const Consts& k) {
+    const T gamma = T(k.gamma);
+    cleft = sqrt(gamma * pleft / rholeft);
+    cright = sqrt(gamma * pright / rhoright);
+    T p1, p2, rho1, c1, c2;
+    if (pleft <= pright) {
+        p1 = pleft; p2 = pright; rho1 = rholeft; c1 = cleft; c2 = cright;
+    } else {
+        p1 = pright; p2 = pleft; rho1 = rhoright; c1 = cright; c2 = cleft;
+    }
+    const T dvv = vxleft - vxright;
+    const T dv2s = (p2 - p1) / sqrt(T(0.5) * rho1 * ((gamma - T(1)) * p1 + (gamma + T(1)) * p2));
+    if (dvv >= dv2s) return 1;
+    const T dv1s = -((T(2) * c2 / (gamma - T(1))) * (T(1) - PowT::pm(p1 / p2, k)));
+    const T dv2r = -(T(2) * (c1 + c2) * T(k.rgamma1));
+    if (dvv < dv2s && dvv >= dv1s) return 2;
+    if (dvv < dv1s && dvv > dv2r) return 3;
+    if (dvv <= dv2r) return 4;
+    return 5;
+}
+
+// FP32 x^m for the mixed classification.
+struct PowF32m {
+    __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, float(k.m)); }
+};
+
+// ------------------------------------------------------------------------
+// riemann, riemann.F90:318-400 (van Leer Newton for p*).  Returns false when
+// more than 100 iterations would be needed (the reference stops the run).
+// ------------------------------------------------------------------------
+template <class Pow>
+__device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, double pleft, double pright,
+                                               double rholeft, double rhoright, double vxleft, double vxright,
+                                               const Consts& k) {
+    double err = 1.e10;
+    int nnewt = 0;
+    const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
+    const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft + vxright);
+    if (pcheck > 0.0) pstar = pcheck;
+    const double cleft = sqrt(k.gamma * pleft * rholeft);
+    const double cright = sqrt(k.gamma * pright * rhoright);
+    while (err > kTerr) {
+        nnewt = nnewt + 1;
+        if (nnewt > kNewtonMax) return false;
+        const double pstarold = pstar;
+        double a, b, vprimel, vprimer;
+        // pstup (:360,:368) is only consulted on the rarefaction side, so the
+        // power is evaluated there alone.
+        const double rl = pstar / pleft, rr = pstar / pright;
+        if (pstar >= pleft) {
+            a = cleft * sqrt(k.gf * pstar / pleft + k.m);
+            vprimel = -((a * a + cleft * cleft) / (2.0 * a * a * a));
+        } else {
+            const double pw = Pow::pm(rl, k);
+            if ((1.0 - pw) == 0.0) a = cleft * sqrt(k.gf * pstar / pleft + k.m);
+            else a = k.m * cleft * (1.0 - pstar / pleft) / (1.0 - pw);
+            vprimel = -((1.0 / cleft) * Pow::pgf(rl, k));
+        }
+        if (pstar >= pright) {
+            b = cright * sqrt(k.gf * pstar / pright + k.m);
+            vprimer = (b * b + cright * cright) / (2.0 * b * b * b);
+        } else {
+            const double pw = Pow::pm(rr, k);
+            if ((1.0 - pw) == 0.0) b = cright * sqrt(k.gf * pstar / pright + k.m);
+            else b = k.m * cright * (1.0 - pstar / pright) / (1.0 - pw);
+            vprimer = (1.0 / cright) * Pow::pgf(rr, k);
+        }
+        const double vstarl = vxleft - (pstar - pleft) / a;
+        const double vstarr = vxright + (pstar - pright) / b;
+        pstar = pstar - (vstarl - vstarr) / (vprimel - vprimer);
+        if (pstar <= 0.0) pstar = pstarold / 1000.0;
+        vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
+        err = fabs(pstarold - pstar) / pstarold;
+    }
+    return true;
+}
+
+// Pattern 1: two shocks, riemannsolver.F90:73-109.
+template <class Pow>
+__device__ __forceinline__ bool riemann_two_shocks(const FaceState& L, const FaceState& R, double& pm, double& vxm,
+                                                   double& rhom, const Consts& k) {
+    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
+    pm = fmax2(pleft, pright);
+    const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+    const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
+    const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
+    double vshock1, vshock2;
+    if (rhoshock1 == rholeft) vshock1 = 0.0;
+    else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
+    if (rhoshock2 == rhoright) vshock2 = 0.0;
+    else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
+    if (vshock2 < 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
+    else if (vxm <= 0.0 && vshock2 >= 0.0) rhom = rhoshock2;
+    else if (vshock1 <= 0.0 && vxm > 0.0) rhom = rhoshock1;
+    else { pm = pleft; vxm = vxleft; rhom = rholeft; }
+    return ok;
+}
+
+// Pattern 2: one shock and one rarefaction, riemannsolver.F90:113-184.
+template <class Pow>
+__device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, const FaceState& R, double cleft,
+                                                          double cright, double& pm, double& vxm, double& rhom,
+                                                          const Consts& k) {
+    const double gamma = k.gamma;
+    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
+    pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
+                      (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
+                  k);
+    const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+    if (pleft >= pright) {
+        const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
+        const double rhocont1 = rholeft * Pow::prg(pm / pleft, k);
+        double vshock2;
+        if (rhoshock2 == rhoright) vshock2 = 0.0;
+        else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
+        const double vtail1 = vxm - sqrt(gamma * pm / rhocont1);
+        const double vhead1 = vxleft - cleft;
+        if (vshock2 < 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
+        else if (vhead1 >= 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
+        else if (vxm <= 0.0 && vshock2 >= 0.0) rhom = rhoshock2;
+        else if (vxm > 0.0 && vtail1 <= 0.0) rhom = rhocont1;
+        else if (vtail1 > 0.0 && vhead1 <= 0.0) {
+            pm = rarwave(pleft, pm, vtail1, vhead1);
+            rhom = rarwave(rholeft, rhocont1, vtail1, vhead1);
+            vxm = rarwave(vxleft, vxm, vtail1, vhead1);
+        }
+    } else {
+        const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
+        const double rhocont2 = rhoright * Pow::prg(pm / pright, k);
+        double vshock1;
+        if (rhoshock1 == rholeft) vshock1 = 0.0;
+        else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
+        const double vtail2 = vxm + sqrt(gamma * pm / rhocont2);
+        const double vhead2 = vxright + cright;
+        if (vshock1 > 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
+        else if (vhead2 <= 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
+        else if (vxm >= 0.0 && vshock1 <= 0.0) rhom = rhoshock1;
+        else if (vxm < 0.0 && vtail2 >= 0.0) rhom = rhocont2;
+        else if (vtail2 < 0.0 && vhead2 >= 0.0) {
+            pm = rarwave(pright, pm, vtail2, vhead2);
+            rhom = rarwave(rhoright, rhocont2, vtail2, vhead2);
+            vxm = rarwave(vxright, vxm, vtail2, vhead2);
+        }
+    }
+    return ok;
+}
+
+// Pattern 3: two rarefactions, riemannsolver.F90:188-227 (closed form).
+// T = double follows the Fortran arithmetic; T = float is the mixed path
+// (no Newton iteration is involved).
+template <class T, class PowT>
+__device__ __forceinline__ void riemann_two_rarefactions(T pleft, T pright, T rholeft, T rhoright, T vxleft,
+                                                         T vxright, T cleft, T cright, T& pm, T& vxm, T& rhom,
+                                                         const Consts& k) {
+    const T gamma = T(k.gamma), rgamma1 = T(k.rgamma1);
+    const T zeta = (cright / cleft) * PowT::pm(pleft / pright, k);
+    const T vtleft = vxleft + T(2) * cleft * rgamma1;
+    const T vtright = vxright - T(2) * cright * rgamma1;
+    vxm = (vtleft * zeta + vtright) / (T(1) + zeta);
+    pm = pleft * PowT::prm((gamma - T(1)) * (vtleft - vtright) / (T(2) * cleft * (T(1) + zeta)), k);
+    const T rhocont1 = rholeft * PowT::prg(pm / pleft, k);
+    const T rhocont2 = rhoright * PowT::prg(pm / pright, k);
+    const T vtail2 = vxm + sqrt(gamma * pm / rhocont2);
+    const T vhead2 = vxright + cright;
+    const T vtail1 = vxm - sqrt(gamma * pm / rhocont1);
+    const T vhead1 = vxleft - cleft;
+    auto rw = [](T f1, T f2, T vt, T vh) { return f2 + vt * (f1 - f2) / (vt - vh); };
+    if (vhead2 <= T(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
+    else if (vhead1 >= T(0)) { pm = pleft; vxm = vxleft; rhom = rholeft; }
+    else if (vhead2 > T(0) && vtail2 <= T(0)) {
+        pm = rw(pright, pm, vtail2, vhead2);
+        rhom = rw(rhoright, rhocont2, vtail2, vhead2);
+        vxm = rw(vxright, vxm, vtail2, vhead2);
+    } else if (vxm <= T(0) && vtail2 > T(0)) rhom = rhocont2;
+    else if (vxm > T(0) && vtail1 <= T(0)) rhom = rhocont1;
+    else if (vtail1 > T(0) && vhead1 <= T(0)) {
+        pm = rw(pleft, pm, vtail1, vhead1);
+        rhom = rw(rholeft, rhocont1, vtail1, vhead1);
+        vxm = rw(vxleft, vxm, vtail1, vhead1);
+    }
+}
+
+// FP32 powers of the two-rarefaction form (mixed path).
+struct PowRareF32 {
+    __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, float(k.m)); }
+    __device__ __forceinline__ static float prm(float x, const Consts& k) {
+        if (k.nroot) {
+            float r = x;
+            for (int i = 1; i < k.nroot; ++i) r *= x;
+            return r;
+        }
+        return PowF32::pw(x, float(k.rm));
+    }
+    __device__ __forceinline__ static float prg(float x, const Consts& k) { return PowF32::pw(x, float(k.rgamma)); }
+};
+
+// Pattern 4: vacuum, riemannsolver.F90:231-264.
+__device__ __forceinline__ void riemann_vacuum(const FaceState& L, const FaceState& R, double cleft, double cright,
+                                               double& pm, double& vxm, double& rhom, const Consts& k) {
+    const double rgamma1 = k.rgamma1;
+    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
+    pm = 0.0;
+    vxm = 0.0;
+    const double rhocont1 = 0.0, rhocont2 = 0.0;
+    const double vtail2 = vxright - 2.0 * cright * rgamma1;
+    const double vhead2 = vxright + cright;
+    const double vtail1 = vxleft - 2.0 * cleft * rgamma1;
+    const double vhead1 = vxleft - cleft;
+    if (vhead2 <= 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
+    else if (vhead1 >= 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
+    else if (vhead2 > 0.0 && vtail2 <= 0.0) {
+        pm = rarwave(pright, pm, vtail2, vhead2);
+        rhom = rarwave(rhoright, rhocont2, vtail2, vhead2);
+        vxm = rarwave(vxright, vxm, vtail2, vhead2);
+    } else if (vtail1 <= 0.0 && vtail2 > 0.0) rhom = 0.0;
+    else if (vtail1 > 0.0 && vhead1 <= 0.0) {
+        pm = rarwave(pleft, pm, vtail1, vhead1);
+        rhom = rarwave(rholeft, rhocont1, vtail1, vhead1);
+        vxm = rarwave(vxleft, vxm, vtail1, vhead1);
+    }
+}
+
+// Transverse velocities upwinded by the sign of u* (riemannsolver.F90:269-275).
+__device__ __forceinline__ void riemann_finish(const FaceState& L, const FaceState& R, double pm, double vxm,
+                                               double rhom, FaceState& out, const StepScalars& s) {
+    const double dadt = 1.0 - 0.5 * s.dat * s.dt * s.rat;  // :36
+    double vym, vzm;
+    if (vxm >= 0.0) { vym = dadt * L.v; vzm = dadt * L.w; }
+    else { vym = dadt * R.v; vzm = dadt * R.w; }
+    out.p = pm; out.rho = rhom; out.u = vxm; out.v = vym; out.w = vzm;
+}
+
+// Solve a face whose pattern is known.  RareT is the arithmetic type of the
+// closed two-rarefaction form (double: FP64 path, float: mixed path).
+template <class Pow, class RareT, class PowRare>
+__device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState& L, const FaceState& R,
+                                                   double cleft, double cright, FaceState& out, const Consts& k,
+                                                   const StepScalars& s) {
+    double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
+    bool ok = true;
+    if (pattern == 1) {
+        ok = riemann_two_shocks<Pow>(L, R, pm, vxm, rhom, k);
+    } else if (pattern == 2) {
+        ok = riemann_shock_rarefaction<Pow>(L, R, cleft, cright, pm, vxm, rhom, k);
+    } else if (pattern == 3) {
+        RareT tp, tv, tr;
+        riemann_two_rarefactions<RareT, PowRare>(RareT(L.p), RareT(R.p), RareT(L.rho), RareT(R.rho), RareT(L.u),
+                                                 RareT(R.u), RareT(cleft), RareT(cright), tp, tv, tr, k);
+        pm = double(tp);
+        vxm = double(tv);
+        rhom = double(tr);
+    } else if (pattern == 4) {
+        riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
+    }
+    riemann_finish(L, R, pm, vxm, rhom, out, s);
+    return ok;
+}
+
+// riemannsolver, riemannsolver.F90:1-285, for a single face in FP64 (the
+// density-peak fix of :279-285 is applied by the caller).
+template <class Pow>
+__device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceState& R, FaceState& out,
+                                              const Consts& k, const StepScalars& s) {
+    double cleft, cright;
+    const int pattern = riemann_classify<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cleft, cright, k);
+    return riemann_by_pattern<Pow, double, Pow>(pattern, L, R, cleft, cright, out, k, s);
+}
+
+}  // namespace hp

@@ -38,6 +38,7 @@
 #pragma once
 #include "hp_device.cuh"
 #include "hp_physics.cuh"
+#include "hp_riemann.cuh"
 
 namespace hp {
 
@@ -57,8 +58,12 @@ struct SweepArgs {
 // Precision policies.  R is the reconstruction/tracing type, Pow the power
 // used by the Riemann solver.
 struct PolicyFP64 {
-    using R = double;
-    using Pow = PowExact;
+    using R = double;          // reconstruction, flattening, tracing
+    using Pow = PowRoot;       // powers of the FP64 Riemann solver
+    using CT = double;         // wave-pattern classification
+    using PowC = PowRoot;
+    using RareT = double;      // closed two-rarefaction form
+    using PowRare = PowRoot;
 };
 
 template <int AXIS>
@@ -94,6 +99,7 @@ struct SweepSmem {
     // Riemann state of face f: each slot is read and then written by the one
     // thread that solves that face
     double rs[5][P * RING];
+    typename Policy::CT cs[2][P * RING];  // Eulerian sound speeds of the face states (classification)
     int work[P * T];            // Riemann problems of the iteration, sorted by pattern
     int cnt[P * T / 32][5];     // per-warp counts of the 5 patterns
     int nwork;
@@ -105,6 +111,7 @@ template <int AXIS, int P, int T, int RING, class Policy>
 __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
     using R = typename Policy::R;
     using Pow = typename Policy::Pow;
+    using CT = typename Policy::CT;
     using L = SweepLayout<AXIS, P, T, RING>;
     static_assert((RING & (RING - 1)) == 0 && RING >= T + 6, "ring too small");
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -336,8 +343,12 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                 S.rs[3][io] = right.v;
                 S.rs[4][io] = right.w;
                 const int il = L::idx(f - 1, tp);
-                mycase = riemann_pattern<Pow>(double(S.ls[0][il]), right.p, double(S.ls[1][il]), right.rho,
-                                              double(S.ls[2][il]), right.u, k);
+                CT cl, cr;
+                mycase = riemann_classify<CT, typename Policy::PowC>(CT(S.ls[0][il]), CT(right.p), CT(S.ls[1][il]),
+                                                                     CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl,
+                                                                     cr, k);
+                S.cs[0][io] = cl;
+                S.cs[1][io] = cr;
             }
             const int lane = tid & 31, warp = tid >> 5;
             const unsigned lt = (1u << lane) - 1u;
@@ -363,7 +374,7 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                     }
                     off += tot;
                 }
-                S.work[off + rank] = (tp << 16) | f;  // (pencil, face) of the problem
+                S.work[off + rank] = (mycase << 24) | (tp << 16) | f;  // (pattern, pencil, face)
             }
             if (tid == 0) {
                 int tot = 0;
@@ -376,7 +387,7 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
         // C2: solve problem number tid of the sorted list.
         if (tid < S.nwork) {
             const int item = S.work[tid];
-            const int wtp = item >> 16, f = item & 0xffff;
+            const int pattern = item >> 24, wtp = (item >> 16) & 0xff, f = item & 0xffff;
             const int il = L::idx(f - 1, wtp), io = L::idx(f, wtp);
             FaceState left, rgt, out;
             left.p = double(S.ls[0][il]);
@@ -389,7 +400,9 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
             rgt.u = S.rs[2][io];
             rgt.v = S.rs[3][io];
             rgt.w = S.rs[4][io];
-            if (!riemannsolver<Pow>(left, rgt, out, k, sc)) status |= kStatNewton;
+            if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare>(
+                    pattern, left, rgt, double(S.cs[0][io]), double(S.cs[1][io]), out, k, sc))
+                status |= kStatNewton;
             // density-peak fix (riemannsolver.F90:279-285)
             if (peak_possible) {
                 double pk;
