@@ -16,7 +16,7 @@ namespace hp {
 
 struct PolicyMixed {
     using R = float;             // reconstruction, flattening, tracing
-    using Pow = PowRoot;         // FP64 Newton for p*, u* (patterns 1, 2) and vacuum
+    using Pow = PowRootShort;    // FP64 Newton for p*, u* (patterns 1, 2) and vacuum
     using CT = float;            // wave-pattern classification
     using PowC = PowF32m;
     using RareT = float;         // closed two-rarefaction form: no iteration

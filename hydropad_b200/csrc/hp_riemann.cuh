@@ -73,6 +73,7 @@ __device__ __forceinline__ double ipow(double y, int n) {
 // x^rgamma = r^j, x^rm = x^n.  These agree with pow() to an ulp or two.
 // Other gammas use pow().
 struct PowRoot {
+    static constexpr bool kShortNewton = false;  // literal riemann.F90 loop body
     __device__ __forceinline__ static double root(double x, const Consts& k) {
         return k.nroot == 5 ? root_fixed<5>(x) : root_any(x, k.nroot);
     }
@@ -88,6 +89,11 @@ struct PowRoot {
     __device__ __forceinline__ static double prm(double x, const Consts& k) {
         return k.nroot ? ipow(x, k.nroot) : pow_shared(x, k.rm);
     }
+};
+
+// The same powers with the shortened Newton loop body (mixed path).
+struct PowRootShort : PowRoot {
+    static constexpr bool kShortNewton = true;
 };
 
 // FP32 powers for the mixed path's closed-form two-rarefaction solution.
@@ -132,10 +138,82 @@ struct PowF32m {
 // riemann, riemann.F90:318-400 (van Leer Newton for p*).  Returns false when
 // more than 100 iterations would be needed (the reference stops the run).
 // ------------------------------------------------------------------------
+// Same iteration with the divisions of the loop body replaced by products
+// with reciprocals formed once (or by rsqrt), and u* formed once after the
+// loop from the last wave speeds: the same sequence of iterates up to
+// rounding, with a shorter dependency chain per iteration.  Used by the
+// mixed-precision path, whose Newton still runs in FP64.
+template <class Pow>
+__device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vstar, double pleft, double pright,
+                                                     double rholeft, double rhoright, double vxleft,
+                                                     double vxright, const Consts& k) {
+    const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
+    const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft + vxright);
+    if (pcheck > 0.0) pstar = pcheck;
+    const double cleft = sqrt(k.gamma * pleft * rholeft);
+    const double cright = sqrt(k.gamma * pright * rhoright);
+    const double rpl = 1.0 / pleft, rpr = 1.0 / pright, rcl = 1.0 / cleft, rcr = 1.0 / cright;
+    double a = 0.0, b = 0.0;
+    for (int nnewt = 1; nnewt <= kNewtonMax; ++nnewt) {
+        const double pstarold = pstar;
+        const double rl = pstar * rpl, rr = pstar * rpr;
+        double ia, ib, vprimel, vprimer;
+        const double rps = 1.0 / pstar;
+        if (pstar >= pleft) {
+            const double q = k.gf * rl + k.m, rs = rsqrt(q);
+            a = cleft * q * rs;
+            ia = rs * rcl;
+            const double ca = cleft * ia;
+            vprimel = -0.5 * ia * (1.0 + ca * ca);
+        } else {
+            const double pw = Pow::pm(rl, k);
+            if ((1.0 - pw) == 0.0) {
+                const double q = k.gf * rl + k.m, rs = rsqrt(q);
+                a = cleft * q * rs;
+                ia = rs * rcl;
+            } else {
+                a = k.m * cleft * (1.0 - rl) / (1.0 - pw);
+                ia = 1.0 / a;
+            }
+            vprimel = -(rcl * pw * pleft * rps);  // (1/cl) rl^-gf = (1/cl) rl^m / rl
+        }
+        if (pstar >= pright) {
+            const double q = k.gf * rr + k.m, rs = rsqrt(q);
+            b = cright * q * rs;
+            ib = rs * rcr;
+            const double cb = cright * ib;
+            vprimer = 0.5 * ib * (1.0 + cb * cb);
+        } else {
+            const double pw = Pow::pm(rr, k);
+            if ((1.0 - pw) == 0.0) {
+                const double q = k.gf * rr + k.m, rs = rsqrt(q);
+                b = cright * q * rs;
+                ib = rs * rcr;
+            } else {
+                b = k.m * cright * (1.0 - rr) / (1.0 - pw);
+                ib = 1.0 / b;
+            }
+            vprimer = rcr * pw * pright * rps;
+        }
+        const double vstarl = vxleft - (pstar - pleft) * ia;
+        const double vstarr = vxright + (pstar - pright) * ib;
+        pstar = pstar - (vstarl - vstarr) / (vprimel - vprimer);
+        if (pstar <= 0.0) pstar = pstarold * 0.001;
+        if (!(fabs(pstarold - pstar) > kTerr * pstarold)) {
+            vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
+            return true;
+        }
+    }
+    vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
+    return false;
+}
+
 template <class Pow>
 __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, double pleft, double pright,
                                                double rholeft, double rhoright, double vxleft, double vxright,
                                                const Consts& k) {
+    if constexpr (Pow::kShortNewton)
+        return riemann_newton_short<Pow>(pstar, vstar, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
     double err = 1.e10;
     int nnewt = 0;
     const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
@@ -335,26 +413,30 @@ __device__ __forceinline__ void riemann_finish(const FaceState& L, const FaceSta
 }
 
 // Solve a face whose pattern is known.  RareT is the arithmetic type of the
-// closed two-rarefaction form (double: FP64 path, float: mixed path).
+// closed two-rarefaction form (double: FP64 path, float: mixed path).  The
+// Eulerian sound speeds (riemannsolver.F90:32-33) are recomputed here, in
+// the type each pattern works in.
 template <class Pow, class RareT, class PowRare>
 __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState& L, const FaceState& R,
-                                                   double cleft, double cright, FaceState& out, const Consts& k,
-                                                   const StepScalars& s) {
+                                                   FaceState& out, const Consts& k, const StepScalars& s) {
     double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
     bool ok = true;
     if (pattern == 1) {
         ok = riemann_two_shocks<Pow>(L, R, pm, vxm, rhom, k);
-    } else if (pattern == 2) {
-        ok = riemann_shock_rarefaction<Pow>(L, R, cleft, cright, pm, vxm, rhom, k);
     } else if (pattern == 3) {
+        const RareT g = RareT(k.gamma);
+        const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);
+        const RareT cleft = sqrt(g * pl / rl), cright = sqrt(g * pr / rr);
         RareT tp, tv, tr;
-        riemann_two_rarefactions<RareT, PowRare>(RareT(L.p), RareT(R.p), RareT(L.rho), RareT(R.rho), RareT(L.u),
-                                                 RareT(R.u), RareT(cleft), RareT(cright), tp, tv, tr, k);
+        riemann_two_rarefactions<RareT, PowRare>(pl, pr, rl, rr, RareT(L.u), RareT(R.u), cleft, cright, tp, tv, tr,
+                                                 k);
         pm = double(tp);
         vxm = double(tv);
         rhom = double(tr);
-    } else if (pattern == 4) {
-        riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
+    } else if (pattern == 2 || pattern == 4) {
+        const double cleft = sqrt(k.gamma * L.p / L.rho), cright = sqrt(k.gamma * R.p / R.rho);
+        if (pattern == 2) ok = riemann_shock_rarefaction<Pow>(L, R, cleft, cright, pm, vxm, rhom, k);
+        else riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
     }
     riemann_finish(L, R, pm, vxm, rhom, out, s);
     return ok;
@@ -367,7 +449,7 @@ __device__ __forceinline__ bool riemannsolver(const FaceState& L, const FaceStat
                                               const Consts& k, const StepScalars& s) {
     double cleft, cright;
     const int pattern = riemann_classify<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cleft, cright, k);
-    return riemann_by_pattern<Pow, double, Pow>(pattern, L, R, cleft, cright, out, k, s);
+    return riemann_by_pattern<Pow, double, Pow>(pattern, L, R, out, k, s);
 }
 
 }  // namespace hp

@@ -99,7 +99,6 @@ struct SweepSmem {
     // Riemann state of face f: each slot is read and then written by the one
     // thread that solves that face
     double rs[5][P * RING];
-    typename Policy::CT cs[2][P * RING];  // Eulerian sound speeds of the face states (classification)
     int work[P * T];            // Riemann problems of the iteration, sorted by pattern
     int cnt[P * T / 32][5];     // per-warp counts of the 5 patterns
     int nwork;
@@ -347,8 +346,6 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
                 mycase = riemann_classify<CT, typename Policy::PowC>(CT(S.ls[0][il]), CT(right.p), CT(S.ls[1][il]),
                                                                      CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl,
                                                                      cr, k);
-                S.cs[0][io] = cl;
-                S.cs[1][io] = cr;
             }
             const int lane = tid & 31, warp = tid >> 5;
             const unsigned lt = (1u << lane) - 1u;
@@ -401,7 +398,7 @@ __global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
             rgt.v = S.rs[3][io];
             rgt.w = S.rs[4][io];
             if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare>(
-                    pattern, left, rgt, double(S.cs[0][io]), double(S.cs[1][io]), out, k, sc))
+                    pattern, left, rgt, out, k, sc))
                 status |= kStatNewton;
             // density-peak fix (riemannsolver.F90:279-285)
             if (peak_possible) {
