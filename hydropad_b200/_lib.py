@@ -50,7 +50,7 @@ EXPORTS = (
     "hp_init", "hp_finalize", "hp_set_scalars", "hp_get_scalars", "hp_attach_state", "hp_sync_to_host",
     "hp_download_state", "hp_ppmsolver", "hp_ppm_lxlylz", "hp_speed", "hp_timedet", "hp_evolve",
     "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count", "hp_set_tiles",
-    "hp_get_tiles", "hp_autotune",
+    "hp_get_tiles", "hp_autotune", "hp_ppmsolver_noalloc",
 )
 
 _lib = None
@@ -90,6 +90,8 @@ def lib():
     L.hp_set_tiles.argtypes = [cp, C.c_int, C.c_int, C.c_int]
     L.hp_get_tiles.argtypes = [cp, ip]
     L.hp_autotune.argtypes = [cp, C.c_int]
+    L.hp_ppmsolver_noalloc.argtypes = [cp, cp, cp, cp, cp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(HpParams), C.POINTER(HpScalars), cp]
     for name in EXPORTS:
         if name not in ("hp_stream", "hp_strerror", "hp_launch_count"):
             getattr(L, name).restype = C.c_int

@@ -26,6 +26,7 @@ SOURCES = [
     # FP32 stages may use the hardware approximations (FP64 is unaffected)
     ("hp_kernels_mixed.cu", ["-use_fast_math"]),
     ("hp_api.cu", []),
+    ("hp_noalloc.cu", []),
 ]
 HEADERS = ["hp_physics.cuh", "hp_riemann.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_sweep_launch.cuh",
            "hp_launch.h"]

@@ -143,6 +143,26 @@ int hp_get_tiles(hp_ctx *ctx, int *tiles /* [3] */);
  * state (reps sweeps each) and keep the fastest. */
 int hp_autotune(hp_ctx *ctx, int reps);
 
+/* One directional sweep (1=x, 2=y, 3=z) on caller-owned DEVICE arrays,
+ * without any device allocation, for callers that cannot allocate (a stream
+ * capture owned by someone else, a foreign memory pool, a host that owns all
+ * device memory).  No counterpart in the reference.
+ *   p..vz: device pointers, dense (nx,ny,nz) interior cells, x fastest,
+ *          periodic; updated in place.  params: namelist values and
+ *          precision; scalars: dt, rdtath, at, dat, rat, ath, dath.
+ *   stream: cudaStream_t (NULL: default stream); the call returns after the
+ *          stream has finished the sweep.
+ * All scratch (control block + density-peak buffer) is one static device
+ * array of 8 MiB + 4 KiB held by every device that loads the library, so
+ * nx*ny*nz may not exceed 1,048,576 cells (HP_ERR_ARG beyond).  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU race. */
+int hp_ppmsolver_noalloc(double *p, double *rho, double *vx, double *vy,
+                         double *vz, int nx, int ny, int nz, int ndirection,
+                         const hp_params *params, const hp_scalars *scalars,
+                         void *stream);
+
 /* Block until the context's stream is idle and return the device status
  * word accumulated since the last call (then cleared). */
 int hp_synchronize(hp_ctx *ctx);
