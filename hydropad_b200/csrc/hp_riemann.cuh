@@ -28,72 +28,77 @@ __device__ __forceinline__ double rhoshock(double p2, double p1, double rho1, do
 // CUDA pow, out of line so that all call sites share one copy of its code.
 static __device__ __noinline__ double pow_shared(double x, double y) { return pow(x, y); }
 
-// x^(1/n) for integer n >= 2: an FP32 estimate (hardware log2/exp2) refined
-// by two Newton steps on y^n = x in FP64.  The FP32 estimate is good to
-// ~2^-22, so two quadratic steps reach the FP64 rounding level.  Inputs
-// outside the FP32 range go to pow().
-template <int N>
-__device__ __forceinline__ double root_fixed(double x) {
-    if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, 1.0 / (double)N);
-    double y = (double)exp2f(__log2f((float)x) * (1.0f / (float)N));
-    constexpr double a = (double)(N - 1) / (double)N, b = 1.0 / (double)N;
-#pragma unroll
-    for (int it = 0; it < 2; ++it) {
-        double yn1 = y;
-#pragma unroll
-        for (int i = 2; i < N; ++i) yn1 *= y;
-        y = a * y + b * x / yn1;
-    }
-    return y;
-}
-
-static __device__ __noinline__ double root_any(double x, int n) {
-    if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, 1.0 / (double)n);
-    double y = (double)exp2f(__log2f((float)x) * (1.0f / (float)n));
-    const double a = (double)(n - 1) / (double)n, b = 1.0 / (double)n;
-#pragma unroll 1
-    for (int it = 0; it < 2; ++it) {
-        double yn1 = y;
-        for (int i = 2; i < n; ++i) yn1 *= y;
-        y = a * y + b * x / yn1;
-    }
-    return y;
-}
-
 __device__ __forceinline__ double ipow(double y, int n) {
     double r = y;
     for (int i = 1; i < n; ++i) r *= y;
     return r;
 }
 
+// z = x^(-1/n) for integer n >= 2, without division: an FP32 estimate
+// (hardware log2/exp2, ~2^-22) refined by two Newton steps on z^-n = x,
+// z <- z + z (1 - x z^n)/n, each of which squares the relative error.  The
+// result is good to a few ulp.  Inputs outside the FP32 range go to pow().
+__device__ __forceinline__ double inv_root(double x, int n) {
+    if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, -1.0 / (double)n);
+    double z = (double)exp2f(__log2f((float)x) * (-1.0f / (float)n));
+    const double rn = 1.0 / (double)n;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) z = z + z * ((1.0 - x * ipow(z, n)) * rn);
+    return z;
+}
+
 // gamma enters the Riemann solver only through m = (gamma-1)/(2 gamma),
 // gf = 1 - m, rgamma and rm = 1/m.  When n = 1/m is an integer (5 for
 // gamma = 5/3; k.nroot) and rgamma = j m with integer j (3 for 5/3; k.jrg),
-// every power is a product of x^(1/n) and x: x^m = r, x^-gf = r/x,
-// x^rgamma = r^j, x^rm = x^n.  These agree with pow() to an ulp or two.
-// Other gammas use pow().
+// every power follows from z = x^(-1/n):  x^-gf = z^(n-1),
+// x^m = x z^(n-1), x^rgamma = (x^m)^j, x^rm = x^n.  These agree with pow()
+// to a few ulp.  Other gammas use pow().
 struct PowRoot {
     static constexpr bool kShortNewton = false;  // literal riemann.F90 loop body
-    __device__ __forceinline__ static double root(double x, const Consts& k) {
-        return k.nroot == 5 ? root_fixed<5>(x) : root_any(x, k.nroot);
-    }
     __device__ __forceinline__ static double pm(double x, const Consts& k) {
-        return k.nroot ? root(x, k) : pow_shared(x, k.m);
+        return k.nroot ? x * ipow(inv_root(x, k.nroot), k.nroot - 1) : pow_shared(x, k.m);
     }
     __device__ __forceinline__ static double pgf(double x, const Consts& k) {
-        return k.nroot ? root(x, k) / x : pow_shared(x, -k.gf);
+        return k.nroot ? ipow(inv_root(x, k.nroot), k.nroot - 1) : pow_shared(x, -k.gf);
+    }
+    // x^m and x^-gf from one root
+    __device__ __forceinline__ static void pm_pgf(double x, double& m_, double& gf_, const Consts& k) {
+        if (k.nroot) {
+            gf_ = ipow(inv_root(x, k.nroot), k.nroot - 1);
+            m_ = x * gf_;
+        } else {
+            m_ = pow_shared(x, k.m);
+            gf_ = pow_shared(x, -k.gf);
+        }
     }
     __device__ __forceinline__ static double prg(double x, const Consts& k) {
-        return (k.nroot && k.jrg) ? ipow(root(x, k), k.jrg) : pow_shared(x, k.rgamma);
+        return (k.nroot && k.jrg) ? ipow(pm(x, k), k.jrg) : pow_shared(x, k.rgamma);
     }
     __device__ __forceinline__ static double prm(double x, const Consts& k) {
         return k.nroot ? ipow(x, k.nroot) : pow_shared(x, k.rm);
     }
+    // IEEE division
+    __device__ __forceinline__ static double div(double a, double b) { return a / b; }
 };
 
-// The same powers with the shortened Newton loop body (mixed path).
+// Mixed path: the shortened Newton loop body, and divisions from the
+// hardware reciprocal estimate refined by two Newton steps plus one
+// residual correction (within an ulp or two of the IEEE quotient).
+__device__ __forceinline__ double rcp_refined(double b) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+    double e = fma(-b, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-b, r, 1.0);
+    return fma(r, e, r);
+}
 struct PowRootShort : PowRoot {
     static constexpr bool kShortNewton = true;
+    __device__ __forceinline__ static double div(double a, double b) {
+        const double r = rcp_refined(b);
+        const double q = a * r;
+        return fma(r, fma(-b, q, a), q);
+    }
 };
 
 // FP32 powers for the mixed path's closed-form two-rarefaction solution.
@@ -152,13 +157,13 @@ __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vsta
     if (pcheck > 0.0) pstar = pcheck;
     const double cleft = sqrt(k.gamma * pleft * rholeft);
     const double cright = sqrt(k.gamma * pright * rhoright);
-    const double rpl = 1.0 / pleft, rpr = 1.0 / pright, rcl = 1.0 / cleft, rcr = 1.0 / cright;
+    const double rpl = Pow::div(1.0, pleft), rpr = Pow::div(1.0, pright);
+    const double rcl = Pow::div(1.0, cleft), rcr = Pow::div(1.0, cright);
     double a = 0.0, b = 0.0;
     for (int nnewt = 1; nnewt <= kNewtonMax; ++nnewt) {
         const double pstarold = pstar;
         const double rl = pstar * rpl, rr = pstar * rpr;
         double ia, ib, vprimel, vprimer;
-        const double rps = 1.0 / pstar;
         if (pstar >= pleft) {
             const double q = k.gf * rl + k.m, rs = rsqrt(q);
             a = cleft * q * rs;
@@ -166,16 +171,17 @@ __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vsta
             const double ca = cleft * ia;
             vprimel = -0.5 * ia * (1.0 + ca * ca);
         } else {
-            const double pw = Pow::pm(rl, k);
+            double pw, pg;
+            Pow::pm_pgf(rl, pw, pg, k);
             if ((1.0 - pw) == 0.0) {
                 const double q = k.gf * rl + k.m, rs = rsqrt(q);
                 a = cleft * q * rs;
                 ia = rs * rcl;
             } else {
-                a = k.m * cleft * (1.0 - rl) / (1.0 - pw);
-                ia = 1.0 / a;
+                ia = Pow::div(1.0 - pw, k.m * cleft * (1.0 - rl));
+                a = Pow::div(k.m * cleft * (1.0 - rl), 1.0 - pw);
             }
-            vprimel = -(rcl * pw * pleft * rps);  // (1/cl) rl^-gf = (1/cl) rl^m / rl
+            vprimel = -(rcl * pg);  // (1/cl) rl^-gf
         }
         if (pstar >= pright) {
             const double q = k.gf * rr + k.m, rs = rsqrt(q);
@@ -184,27 +190,28 @@ __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vsta
             const double cb = cright * ib;
             vprimer = 0.5 * ib * (1.0 + cb * cb);
         } else {
-            const double pw = Pow::pm(rr, k);
+            double pw, pg;
+            Pow::pm_pgf(rr, pw, pg, k);
             if ((1.0 - pw) == 0.0) {
                 const double q = k.gf * rr + k.m, rs = rsqrt(q);
                 b = cright * q * rs;
                 ib = rs * rcr;
             } else {
-                b = k.m * cright * (1.0 - rr) / (1.0 - pw);
-                ib = 1.0 / b;
+                ib = Pow::div(1.0 - pw, k.m * cright * (1.0 - rr));
+                b = Pow::div(k.m * cright * (1.0 - rr), 1.0 - pw);
             }
-            vprimer = rcr * pw * pright * rps;
+            vprimer = rcr * pg;
         }
         const double vstarl = vxleft - (pstar - pleft) * ia;
         const double vstarr = vxright + (pstar - pright) * ib;
-        pstar = pstar - (vstarl - vstarr) / (vprimel - vprimer);
+        pstar = pstar - Pow::div(vstarl - vstarr, vprimel - vprimer);
         if (pstar <= 0.0) pstar = pstarold * 0.001;
         if (!(fabs(pstarold - pstar) > kTerr * pstarold)) {
-            vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
+            vstar = Pow::div(pleft - pright + a * vxleft + b * vxright, a + b);
             return true;
         }
     }
-    vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
+    vstar = Pow::div(pleft - pright + a * vxleft + b * vxright, a + b);
     return false;
 }
 
@@ -233,19 +240,21 @@ __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, dou
             a = cleft * sqrt(k.gf * pstar / pleft + k.m);
             vprimel = -((a * a + cleft * cleft) / (2.0 * a * a * a));
         } else {
-            const double pw = Pow::pm(rl, k);
+            double pw, pg;
+            Pow::pm_pgf(rl, pw, pg, k);
             if ((1.0 - pw) == 0.0) a = cleft * sqrt(k.gf * pstar / pleft + k.m);
             else a = k.m * cleft * (1.0 - pstar / pleft) / (1.0 - pw);
-            vprimel = -((1.0 / cleft) * Pow::pgf(rl, k));
+            vprimel = -((1.0 / cleft) * pg);
         }
         if (pstar >= pright) {
             b = cright * sqrt(k.gf * pstar / pright + k.m);
             vprimer = (b * b + cright * cright) / (2.0 * b * b * b);
         } else {
-            const double pw = Pow::pm(rr, k);
+            double pw, pg;
+            Pow::pm_pgf(rr, pw, pg, k);
             if ((1.0 - pw) == 0.0) b = cright * sqrt(k.gf * pstar / pright + k.m);
             else b = k.m * cright * (1.0 - pstar / pright) / (1.0 - pw);
-            vprimer = (1.0 / cright) * Pow::pgf(rr, k);
+            vprimer = (1.0 / cright) * pg;
         }
         const double vstarl = vxleft - (pstar - pleft) / a;
         const double vstarr = vxright + (pstar - pright) / b;
