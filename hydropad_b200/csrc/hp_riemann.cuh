@@ -38,13 +38,33 @@ __device__ __forceinline__ double ipow(double y, int n) {
 // (hardware log2/exp2, ~2^-22) refined by two Newton steps on z^-n = x,
 // z <- z + z (1 - x z^n)/n, each of which squares the relative error.  The
 // result is good to a few ulp.  Inputs outside the FP32 range go to pow().
-__device__ __forceinline__ double inv_root(double x, int n) {
+template <int N>
+__device__ __forceinline__ double ipow_fixed(double y) {
+    double r = y;
+#pragma unroll
+    for (int i = 1; i < N; ++i) r *= y;
+    return r;
+}
+template <int N>
+__device__ __forceinline__ double inv_root_fixed(double x) {
+    if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, -1.0 / (double)N);
+    double z = (double)exp2f(__log2f((float)x) * (-1.0f / (float)N));
+    constexpr double rn = 1.0 / (double)N;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) z = z + z * ((1.0 - x * ipow_fixed<N>(z)) * rn);
+    return z;
+}
+static __device__ __noinline__ double inv_root_any(double x, int n) {
     if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, -1.0 / (double)n);
     double z = (double)exp2f(__log2f((float)x) * (-1.0f / (float)n));
     const double rn = 1.0 / (double)n;
-#pragma unroll
     for (int it = 0; it < 2; ++it) z = z + z * ((1.0 - x * ipow(z, n)) * rn);
     return z;
+}
+// x^(-(n-1)/n) = x^-gf, the common factor of every power below
+__device__ __forceinline__ double pow_mgf(double x, int n) {
+    if (n == 5) return ipow_fixed<4>(inv_root_fixed<5>(x));
+    return ipow(inv_root_any(x, n), n - 1);
 }
 
 // gamma enters the Riemann solver only through m = (gamma-1)/(2 gamma),
@@ -56,15 +76,15 @@ __device__ __forceinline__ double inv_root(double x, int n) {
 struct PowRoot {
     static constexpr bool kShortNewton = false;  // literal riemann.F90 loop body
     __device__ __forceinline__ static double pm(double x, const Consts& k) {
-        return k.nroot ? x * ipow(inv_root(x, k.nroot), k.nroot - 1) : pow_shared(x, k.m);
+        return k.nroot ? x * pow_mgf(x, k.nroot) : pow_shared(x, k.m);
     }
     __device__ __forceinline__ static double pgf(double x, const Consts& k) {
-        return k.nroot ? ipow(inv_root(x, k.nroot), k.nroot - 1) : pow_shared(x, -k.gf);
+        return k.nroot ? pow_mgf(x, k.nroot) : pow_shared(x, -k.gf);
     }
     // x^m and x^-gf from one root
     __device__ __forceinline__ static void pm_pgf(double x, double& m_, double& gf_, const Consts& k) {
         if (k.nroot) {
-            gf_ = ipow(inv_root(x, k.nroot), k.nroot - 1);
+            gf_ = pow_mgf(x, k.nroot);
             m_ = x * gf_;
         } else {
             m_ = pow_shared(x, k.m);
@@ -72,9 +92,11 @@ struct PowRoot {
         }
     }
     __device__ __forceinline__ static double prg(double x, const Consts& k) {
+        if (k.nroot == 5 && k.jrg == 3) return ipow_fixed<3>(pm(x, k));
         return (k.nroot && k.jrg) ? ipow(pm(x, k), k.jrg) : pow_shared(x, k.rgamma);
     }
     __device__ __forceinline__ static double prm(double x, const Consts& k) {
+        if (k.nroot == 5) return ipow_fixed<5>(x);
         return k.nroot ? ipow(x, k.nroot) : pow_shared(x, k.rm);
     }
     // IEEE division
@@ -375,6 +397,7 @@ __device__ __forceinline__ void riemann_two_rarefactions(T pleft, T pright, T rh
 struct PowRareF32 {
     __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, float(k.m)); }
     __device__ __forceinline__ static float prm(float x, const Consts& k) {
+        if (k.nroot == 5) return x * x * x * x * x;
         if (k.nroot) {
             float r = x;
             for (int i = 1; i < k.nroot; ++i) r *= x;
