@@ -165,6 +165,7 @@ def run_ours(args):
     for prec in ("fp64", "mixed"):
         h = Hydro(prm, precision=prec, device=local)
         h.attach_state(*state)
+        tiles = h.autotune(reps=2)  # tile shape per axis, timed on a scratch copy
         h.start_with_cfl()
         h.evolve(W, graph=True)
         stream = torch.cuda.ExternalStream(h.stream_handle())
@@ -182,7 +183,7 @@ def run_ours(args):
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1)) / K
         results[prec] = {"ms_per_step": ms, "value": world * cells / (ms * 1e-3),
-                         "launches": h.launch_count() - l0, "clocks": clk.summary()}
+                         "launches": h.launch_count() - l0, "clocks": clk.summary(), "tiles": tiles}
         finals[prec] = h.download(nbound=0)
         # per-sweep duration of the dominant kernel (fused sweep), CUDA events
         # on the launching stream; 3 sweeps per ppm_lxlylz call
@@ -210,6 +211,7 @@ def run_ours(args):
             hst[...] = src
         h = Hydro(prm, precision="mixed", device=local)
         h.attach_state(*host)
+        h.set_tiles(*results["mixed"]["tiles"])
         h.start_with_cfl()
         h.evolve(1, graph=True)
         h.sync_to_host()
@@ -259,6 +261,7 @@ def run_ours(args):
         "data": "synthetic (seeded GRF initial conditions)",
         "config": workload_config(n, world, "mixed"),
         "fp64": {"value": fp["value"], "ms_per_step": fp["ms_per_step"], "sweep_ms": fp["sweep_ms"],
+                 "tiles": fp["tiles"],
                  "roofline_frac": BYTES_PER_CELL_SWEEP * cells / (fp["sweep_ms"] * 1e-3) / 1e9 / peaks[0]},
         "mixed_over_fp64": mx["value"] / fp["value"],
         "density_rel_l1_mixed_vs_fp64": dens_l1,
@@ -268,6 +271,7 @@ def run_ours(args):
                      "kernel": "ppm_sweep_kernel (mixed)",
                      "algorithmic_bytes_per_launch": BYTES_PER_CELL_SWEEP * cells},
         "gpu_launches": mx["launches"],
+        "tiles": mx["tiles"],
         "clocks": mx["clocks"],
         "e2e": e2e,
         "cpu_baseline": cpu,

@@ -25,6 +25,6 @@ int launch_speed(const Box& b, cudaStream_t st);
 int launch_timedet(const Box& b, int advance, cudaStream_t st);
 
 // Number of tile shapes per axis (hp_sweep_launch.cuh).
-constexpr int kNumTiles = 6;
+constexpr int kNumTiles = 8;
 
 }  // namespace hp

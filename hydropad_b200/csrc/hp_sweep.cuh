@@ -106,8 +106,11 @@ struct SweepSmem {
     unsigned long long red[128];
 };
 
-template <int AXIS, int P, int T, int RING, class Policy>
-__global__ void __launch_bounds__(P* T) ppm_sweep_kernel(SweepArgs a) {
+// MINB > 1 asks the compiler for at most 65536/(P*T*MINB) registers per
+// thread so that MINB CTAs fit on one SM (more warps to hide the latency of
+// the FP64 Riemann chains, at the price of spills).
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
+__global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
     using R = typename Policy::R;
     using Pow = typename Policy::Pow;
     using CT = typename Policy::CT;

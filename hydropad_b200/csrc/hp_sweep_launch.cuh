@@ -13,9 +13,9 @@
 
 namespace hp {
 
-constexpr int kTilesX = 6, kTilesYZ = 6;
+constexpr int kTilesX = 8, kTilesYZ = 8;
 
-template <int AXIS, int P, int T, int RING, class Policy>
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
 static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
     SweepArgs a;
     // permute velocities into (normal, transverse1, transverse2) of this
@@ -35,7 +35,7 @@ static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
     a.bslot = bslot;
     a.flags = flags;
     const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy>);
-    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy>;
+    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB>;
     static bool attr_set = false;  // per instantiation (one process drives one device)
     if (!attr_set) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -57,6 +57,8 @@ static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int 
             case 3: return launch_sweep_t<0, 4, 16, 32, Policy>(b, bslot, flags, st);
             case 4: return launch_sweep_t<0, 16, 32, 64, Policy>(b, bslot, flags, st);
             case 5: return launch_sweep_t<0, 12, 32, 64, Policy>(b, bslot, flags, st);
+            case 6: return launch_sweep_t<0, 8, 32, 64, Policy, 3>(b, bslot, flags, st);
+            case 7: return launch_sweep_t<0, 4, 32, 64, Policy, 5>(b, bslot, flags, st);
         }
     } else if (axis == 1) {
         switch (tile) {
@@ -66,6 +68,8 @@ static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int 
             case 3: return launch_sweep_t<1, 16, 4, 16, Policy>(b, bslot, flags, st);
             case 4: return launch_sweep_t<1, 64, 8, 16, Policy>(b, bslot, flags, st);
             case 5: return launch_sweep_t<1, 32, 12, 32, Policy>(b, bslot, flags, st);
+            case 6: return launch_sweep_t<1, 32, 8, 16, Policy, 3>(b, bslot, flags, st);
+            case 7: return launch_sweep_t<1, 16, 8, 16, Policy, 5>(b, bslot, flags, st);
         }
     } else if (axis == 2) {
         switch (tile) {
@@ -75,6 +79,8 @@ static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int 
             case 3: return launch_sweep_t<2, 16, 4, 16, Policy>(b, bslot, flags, st);
             case 4: return launch_sweep_t<2, 64, 8, 16, Policy>(b, bslot, flags, st);
             case 5: return launch_sweep_t<2, 32, 12, 32, Policy>(b, bslot, flags, st);
+            case 6: return launch_sweep_t<2, 32, 8, 16, Policy, 3>(b, bslot, flags, st);
+            case 7: return launch_sweep_t<2, 16, 8, 16, Policy, 5>(b, bslot, flags, st);
         }
     }
     return -1;

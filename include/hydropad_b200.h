@@ -132,7 +132,7 @@ int hp_timedet(hp_ctx *ctx, double velmax);
  * them.  Returns the accumulated error status. */
 int hp_evolve(hp_ctx *ctx, int nsteps, int use_graph);
 
-/* Sweep tile shape per axis (0 .. 5; pencils per CTA x cells per window
+/* Sweep tile shape per axis (0 .. 7; pencils per CTA x cells per window
  * step).  Results do not depend on the tile, only the speed does.  No
  * reference counterpart (the reference leaves the launch shape to PGI's
  * OpenACC compiler, ppmsolver.F90:96 `!num_gangs ... vector_length`). */
