@@ -51,7 +51,12 @@ EXPORTS = (
     "hp_download_state", "hp_ppmsolver", "hp_ppm_lxlylz", "hp_speed", "hp_timedet", "hp_evolve",
     "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count", "hp_set_tiles",
     "hp_get_tiles", "hp_autotune", "hp_ppmsolver_noalloc",
+    "hp_batch_create", "hp_batch_destroy", "hp_batch_add", "hp_batch_remove", "hp_batch_size",
+    "hp_batch_step", "hp_batch_synchronize", "hp_batch_member", "hp_batch_set_tiles", "hp_batch_get_tiles",
+    "hp_batch_autotune", "hp_batch_stream", "hp_batch_launch_count",
 )
+_NOT_INT = ("hp_stream", "hp_strerror", "hp_launch_count", "hp_batch_member", "hp_batch_stream",
+            "hp_batch_launch_count")
 
 _lib = None
 
@@ -92,8 +97,24 @@ def lib():
     L.hp_autotune.argtypes = [cp, C.c_int]
     L.hp_ppmsolver_noalloc.argtypes = [cp, cp, cp, cp, cp, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.POINTER(HpParams), C.POINTER(HpScalars), cp]
+    L.hp_batch_create.argtypes = [C.POINTER(cp), C.c_int, C.c_int, C.c_int]
+    L.hp_batch_destroy.argtypes = [cp]
+    L.hp_batch_add.argtypes = [cp, cp]
+    L.hp_batch_remove.argtypes = [cp, cp]
+    L.hp_batch_size.argtypes = [cp]
+    L.hp_batch_step.argtypes = [cp, C.c_int, C.c_int]
+    L.hp_batch_synchronize.argtypes = [cp, ip]
+    L.hp_batch_member.argtypes = [cp, C.c_int]
+    L.hp_batch_member.restype = cp
+    L.hp_batch_set_tiles.argtypes = [cp, C.c_int, C.c_int, C.c_int]
+    L.hp_batch_get_tiles.argtypes = [cp, ip]
+    L.hp_batch_autotune.argtypes = [cp, C.c_int]
+    L.hp_batch_stream.argtypes = [cp]
+    L.hp_batch_stream.restype = cp
+    L.hp_batch_launch_count.argtypes = [cp]
+    L.hp_batch_launch_count.restype = C.c_longlong
     for name in EXPORTS:
-        if name not in ("hp_stream", "hp_strerror", "hp_launch_count"):
+        if name not in _NOT_INT:
             getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -1,9 +1,11 @@
 """Build recipe of the CUDA library (libhydropad_b200.so, in-tree).
 
-Every kernel is compiled for sm_100a only.  The FP64 kernels are compiled
-without multiply-add contraction (--fmad=false) so that they round like the
-reference's scalar Fortran; the mixed-precision kernels and the host code use
-the default.
+Every kernel is compiled for sm_100a only, without implicit multiply-add
+contraction (--fmad=false): the FP64 kernels then round like the reference's
+scalar Fortran, and every kernel gives the same bits in every tile shape and
+in batched launches.  The mixed-precision kernels also use the hardware
+approximations of FP32 division and square root (-use_fast_math); fused
+multiply-adds there are written explicitly.
 """
 from __future__ import annotations
 
@@ -11,6 +13,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -21,15 +24,23 @@ LIB_PATH = os.path.join(HERE, LIB_NAME)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
+MIXED = ["-use_fast_math", "--fmad=false"]
 SOURCES = [
     ("hp_kernels_fp64.cu", ["--fmad=false"]),
-    # FP32 stages may use the hardware approximations (FP64 is unaffected)
-    ("hp_kernels_mixed.cu", ["-use_fast_math"]),
+    # FP32 stages may use the hardware approximations (FP64 is unaffected).
+    # No implicit contraction either: ptxas may contract a multiply-add
+    # differently in different instantiations (tiles, batched or not), and
+    # a box must give the same bits whatever tile or batch it runs in.
+    ("hp_kernels_mixed.cu", MIXED),
+    # persistent batched sweeps (many boxes per launch), same flags as above
+    ("hp_batch_fp64.cu", ["--fmad=false"]),
+    ("hp_batch_mixed.cu", MIXED),
     ("hp_api.cu", []),
+    ("hp_batch.cu", []),
     ("hp_noalloc.cu", []),
 ]
 HEADERS = ["hp_physics.cuh", "hp_riemann.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_sweep_launch.cuh",
-           "hp_launch.h"]
+           "hp_launch.h", "hp_ctx.h"]
 
 
 def _nvcc() -> str:
@@ -50,6 +61,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     deps = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "hydropad_b200.h")]
     newest_dep = max(_mtime(d) for d in deps)
     objs = []
+    cmds = []
     relink = force or not os.path.exists(LIB_PATH)
     for src, extra in SOURCES:
         s = os.path.join(CSRC, src)
@@ -60,8 +72,15 @@ def build(verbose: bool = False, force: bool = False) -> str:
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
                 print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
-            relink = True
+            cmds.append(cmd)
+    # translation units compile independently: one nvcc per unit
+    if cmds:
+        with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+            for r in list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds)):
+                sys.stderr.write(r.stderr)
+                if r.returncode != 0:
+                    raise subprocess.CalledProcessError(r.returncode, r.args, r.stdout, r.stderr)
+        relink = True
     if relink or _mtime(LIB_PATH) < max(_mtime(o) for o in objs):
         cmd = [nvcc, *ARCH, "-shared", "-o", LIB_PATH, *objs]
         if verbose:

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/hydropad_b200.h"
+#include "hp_ctx.h"
 #include "hp_device.cuh"
 #include "hp_launch.h"
 
@@ -25,22 +26,6 @@ int launch_sweep(const Box& b, int axis, int tile, int bslot, int flags, int pre
 }
 }  // namespace hp
 
-struct hp_ctx {
-    hp_params prm;
-    int dev;
-    cudaStream_t stream;
-    hp::Box box;
-    hp::DevCtl* ctl_pinned;   // host mirror for reads
-    long long sweep_count;    // selects the rho-bound slot
-    long long nstep_host;     // host mirror of the step counter (selects nrot)
-    const double* host[5];    // attached host arrays (ghosted, Fortran order)
-    int hnx, hny, hnz, hnb;
-    bool attached;
-    int tile[3];              // sweep tile shape per axis (hp_set_tiles / hp_autotune)
-    cudaGraphExec_t graph[6][3];
-    int graph_kernels[6][3];
-    long long launches;
-};
 
 namespace {
 
@@ -59,13 +44,6 @@ int cuda_fail(cudaError_t e) {
         cudaError_t e_ = (x);                            \
         if (e_ != cudaSuccess) return cuda_fail(e_);     \
     } while (0)
-
-int status_to_err(unsigned st) {
-    if (st & hp::kStatNewton) return HP_ERR_NEWTON;
-    if (st & hp::kStatNaN) return HP_ERR_NAN;
-    if (st & hp::kStatNegative) return HP_ERR_NEGATIVE_STATE;
-    return HP_OK;
-}
 
 // initialize_parameters.F90:133-205 on a host DevCtl.
 void init_time(const hp_params& p, hp::DevCtl& c) {
@@ -171,26 +149,14 @@ int do_sweep(hp_ctx* x, int axis, int flags) {
     return HP_OK;
 }
 
-const int kOrder[6][3] = {{0, 1, 2}, {2, 1, 0}, {1, 2, 0}, {0, 2, 1}, {2, 0, 1}, {1, 0, 2}};  // ppm_lxlylz.F90
-
 // One evolve_sys step on the device: three sweeps (the first snapshots the
 // state for expand, the last applies expand and accumulates velmax) and
 // timedet.  Returns the number of kernels or a negative error.
 int enqueue_step(hp_ctx* x, int nrot) {
-    const bool cosmo = x->prm.cosmo != 0;
     int kern = 0;
     for (int s = 0; s < 3; ++s) {
-        int flags = 0;
-        if (s == 0) {
-            flags |= hp::kFlagResetSpeed;
-            if (cosmo && !x->prm.expand_zero_old) flags |= hp::kFlagSnapshot;
-        }
-        if (s == 2) {
-            flags |= hp::kFlagSpeed;
-            if (cosmo) flags |= hp::kFlagExpand | (x->prm.expand_zero_old ? hp::kFlagExpandZeroOld : 0);
-        }
         const long long before = x->launches;
-        const int rc = do_sweep(x, kOrder[nrot - 1][s], flags);
+        const int rc = do_sweep(x, hp::kSweepOrder[nrot - 1][s], hp::step_flags(x->prm, s));
         if (rc != HP_OK) return rc;
         kern += (int)(x->launches - before);
     }
@@ -422,7 +388,7 @@ int hp_ppm_lxlylz(hp_ctx* x, int nrot) {
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     HP_CUDA(cudaSetDevice(x->dev));
     for (int s = 0; s < 3; ++s) {
-        int rc = do_sweep(x, kOrder[nrot - 1][s], 0);
+        int rc = do_sweep(x, hp::kSweepOrder[nrot - 1][s], 0);
         if (rc != HP_OK) return rc;
     }
     return HP_OK;
@@ -458,8 +424,7 @@ int hp_evolve(hp_ctx* x, int nsteps, int use_graph) {
     HP_CUDA(cudaSetDevice(x->dev));
     for (int it = 0; it < nsteps; ++it) {
         const long long nstep = x->nstep_host;
-        int nrot = (int)(nstep % 6) + 1;  // evolve_sys.F90:30-31
-        if (nstep == 1) nrot = 1;
+        const int nrot = hp::nrot_of_step(nstep);
         const int slot = (int)(x->sweep_count % 3);
         if (!use_graph) {
             const int n = enqueue_step(x, nrot);
@@ -496,7 +461,7 @@ int hp_synchronize(hp_ctx* x) {
     HP_CUDA(cudaMemcpyAsync(&st, &x->box.ctl->status, sizeof st, cudaMemcpyDeviceToHost, x->stream));
     HP_CUDA(cudaMemsetAsync(&x->box.ctl->status, 0, sizeof st, x->stream));
     HP_CUDA(cudaStreamSynchronize(x->stream));
-    return status_to_err(st);
+    return hp::status_error(st);
 }
 
 void* hp_stream(hp_ctx* x) { return x ? (void*)x->stream : nullptr; }

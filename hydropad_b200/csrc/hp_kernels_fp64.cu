@@ -84,7 +84,7 @@ constexpr double kC0P1 = 0.10000000149011612;   // 0.1 (functions.F90:80,155)
 constexpr double kTwo3 = 0.6666666865348816;    // 2.0/3.0 as REAL(4)
 constexpr double kMThird = -0.3333333432674408; // -1.0/3.0 as REAL(4)
 
-__global__ void timedet_kernel(DevCtl* c, int advance) {
+__device__ void timedet_one(DevCtl* c, int advance) {
     if (c->done) return;
     const double velmax = __longlong_as_double((long long)c->velmax_key);
     c->velmax = velmax;
@@ -136,6 +136,35 @@ __global__ void timedet_kernel(DevCtl* c, int advance) {
     if (!(c->told < c->tstop)) c->done = 1;
 }
 
+__global__ void timedet_kernel(DevCtl* c, int advance) { timedet_one(c, advance); }
+
+// One thread per box of a batch, at the end of a step.
+__global__ void timedet_batch_kernel(DevCtl* const* __restrict__ ctls, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) timedet_one(ctls[i], 1);
+}
+
+int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st) {
+    if (n <= 0) return 0;
+    timedet_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(ctls, n);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+// Status words of a batch's boxes into out[], each cleared.
+__global__ void status_gather_kernel(DevCtl* const* __restrict__ ctls, int n, unsigned* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        out[i] = ctls[i]->status;
+        ctls[i]->status = 0u;
+    }
+}
+
+int launch_status_gather(DevCtl* const* ctls, int n, unsigned* out, cudaStream_t st) {
+    if (n <= 0) return 0;
+    status_gather_kernel<<<(n + 127) / 128, 128, 0, st>>>(ctls, n, out);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
 int launch_timedet(const Box& b, int advance, cudaStream_t st) {
     timedet_kernel<<<1, 1, 0, st>>>(b.ctl, advance);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
@@ -151,13 +180,14 @@ int launch_timedet(const Box& b, int advance, cudaStream_t st) {
 // state.  Indices wrap periodically (identical to the reference's ghost
 // reads for cubic boxes).  Runs only when the rho bounds admit a peak.
 // ---------------------------------------------------------------------------
-__global__ void peak_prepass_kernel(const double* __restrict__ rho, const double* __restrict__ vn, double* peak,
-                                    int nx, int ny, int nz, int axis, double dmax, const DevCtl* c, int bslot) {
+__device__ __forceinline__ void peak_prepass_box(const double* __restrict__ rho, const double* __restrict__ vn,
+                                                 double* peak, int nx, int ny, int nz, int axis, double dmax,
+                                                 const DevCtl* c, int bslot, long long i0, long long di) {
     const double rmin0 = dkey_decode(c->rho_key[bslot][0]);
     const double rmax0 = dkey_decode(c->rho_key[bslot][1]);
     if (!(rmax0 > dmax * rmin0) || c->done) return;
     const long long n = (long long)nx * ny * nz;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = i0; i < n; i += di) {
         const int x = (int)(i % nx);
         const int y = (int)((i / nx) % ny);
         const int z = (int)(i / ((long long)nx * ny));
@@ -170,6 +200,26 @@ __global__ void peak_prepass_kernel(const double* __restrict__ rho, const double
         auto at = [&](int o) { int xi = ((f + o) % nx + nx) % nx; return row + xi; };
         peak[i] = peak_value(rho[at(-3)], rho[at(-2)], rho[at(-1)], rho[at(0)], vn[at(-2)], vn[at(-1)], dmax);
     }
+}
+
+__global__ void peak_prepass_kernel(const double* __restrict__ rho, const double* __restrict__ vn, double* peak,
+                                    int nx, int ny, int nz, int axis, double dmax, const DevCtl* c, int bslot) {
+    peak_prepass_box(rho, vn, peak, nx, ny, nz, axis, dmax, c, bslot,
+                     blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
+// Batch form: blockIdx.y selects the entry (box) of a batched y/z sweep.
+__global__ void peak_prepass_batch_kernel(BatchLaunch bl, int axis) {
+    const SweepArgs& a = bl.args[bl.ent[blockIdx.y]];
+    if (a.peak == nullptr) return;
+    peak_prepass_box(a.f[1], a.f[2], const_cast<double*>(a.peak), a.nx, a.ny, a.nz, axis, a.k.dmax, a.ctl, a.bslot,
+                     blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
+int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st) {
+    if (axis == 0 || bl.nent <= 0) return 0;
+    peak_prepass_batch_kernel<<<dim3(64, bl.nent), 256, 0, st>>>(bl, axis);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
 int launch_peak_prepass(const Box& b, int axis, int bslot, cudaStream_t st) {

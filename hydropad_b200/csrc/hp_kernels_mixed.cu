@@ -14,15 +14,6 @@
 
 namespace hp {
 
-struct PolicyMixed {
-    using R = float;             // reconstruction, flattening, tracing
-    using Pow = PowRootShort;    // FP64 Newton for p*, u* (patterns 1, 2) and vacuum
-    using CT = float;            // wave-pattern classification
-    using PowC = PowF32m;
-    using RareT = float;         // closed two-rarefaction form: no iteration
-    using PowRare = PowRareF32;
-};
-
 int launch_sweep_mixed(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
     return launch_sweep_policy<PolicyMixed>(b, axis, tile, bslot, flags, st);
 }

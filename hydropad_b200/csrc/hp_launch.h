@@ -24,7 +24,22 @@ int launch_bounds(const Box& b, int slot, cudaStream_t st);
 int launch_speed(const Box& b, cudaStream_t st);
 int launch_timedet(const Box& b, int advance, cudaStream_t st);
 
-// Number of tile shapes per axis (hp_sweep_launch.cuh).
+// Number of tile shapes per axis, and the pencils per CTA (P) of each
+// (the tile table in hp_sweep_launch.cuh).
 constexpr int kNumTiles = 8;
+constexpr int kTilePencils[3][kNumTiles] = {
+    {8, 4, 8, 4, 16, 12, 8, 4}, {32, 16, 32, 16, 64, 32, 32, 16}, {32, 16, 32, 16, 64, 32, 32, 16}};
+
+struct BatchLaunch;  // hp_sweep.cuh
+
+// Batched sweep over many boxes (one axis per launch); the counter must be
+// zero when the launch starts.
+int launch_sweep_batch(const BatchLaunch& bl, int axis, int tile, int precision, cudaStream_t st);
+// Peak pre-pass of the boxes of one y/z batch launch.
+int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st);
+// timedet (advance = 1) on n control blocks.
+int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st);
+// out[i] = status word of ctls[i], which is cleared.
+int launch_status_gather(DevCtl* const* ctls, int n, unsigned* out, cudaStream_t st);
 
 }  // namespace hp

@@ -459,12 +459,27 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
         const RareT g = RareT(k.gamma);
         const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);
         const RareT cleft = sqrt(g * pl / rl), cright = sqrt(g * pr / rr);
-        RareT tp, tv, tr;
+        // NaN when no branch of the closed form applies (a NaN state), as
+        // the undefined values of the reference
+        RareT tp = RareT(pm), tv = tp, tr = tp;
         riemann_two_rarefactions<RareT, PowRare>(pl, pr, rl, rr, RareT(L.u), RareT(R.u), cleft, cright, tp, tv, tr,
                                                  k);
         pm = double(tp);
         vxm = double(tv);
         rhom = double(tr);
+        if constexpr (sizeof(RareT) < sizeof(double)) {
+            // A face at the edge of the vacuum condition (the FP32
+            // classification said two rarefactions, the FP32 closed form
+            // gives a non-positive star pressure or density, or one below
+            // FP32's range): classify and solve it again in FP64.
+            if (!(pm > 0.0 && rhom > 0.0 && vxm == vxm)) {
+                double cl, cr;
+                const int p64 = riemann_classify<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cl, cr, k);
+                pm = vxm = rhom = __longlong_as_double(0x7ff8000000000000ULL);
+                if (p64 == 4) riemann_vacuum(L, R, cl, cr, pm, vxm, rhom, k);
+                else riemann_two_rarefactions<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cl, cr, pm, vxm, rhom, k);
+            }
+        }
     } else if (pattern == 2 || pattern == 4) {
         const double cleft = sqrt(k.gamma * L.p / L.rho), cright = sqrt(k.gamma * R.p / R.rho);
         if (pattern == 2) ok = riemann_shock_rarefaction<Pow>(L, R, cleft, cright, pm, vxm, rhom, k);

@@ -65,6 +65,18 @@ struct PolicyFP64 {
     using RareT = double;      // closed two-rarefaction form
     using PowRare = PowRoot;
 };
+// Mixed precision: reconstruction, flattening, characteristic tracing and
+// the traced face states in FP32; the Riemann solver's Newton for p*, u*,
+// the conservative update and the dual-energy switch in FP64; the state in
+// HBM stays FP64.
+struct PolicyMixed {
+    using R = float;             // reconstruction, flattening, tracing
+    using Pow = PowRootShort;    // FP64 Newton for p*, u* (patterns 1, 2) and vacuum
+    using CT = float;            // wave-pattern classification
+    using PowC = PowF32m;
+    using RareT = float;         // closed two-rarefaction form: no iteration
+    using PowRare = PowRareF32;
+};
 
 template <int AXIS>
 __device__ __forceinline__ long long pencil_base(long long pid, int nx, int ny) {
@@ -106,23 +118,21 @@ struct SweepSmem {
     unsigned long long red[128];
 };
 
-// MINB > 1 asks the compiler for at most 65536/(P*T*MINB) registers per
-// thread so that MINB CTAs fit on one SM (more warps to hide the latency of
-// the FP64 Riemann chains, at the price of spills).
-template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
-__global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
+// One CTA's worth of work: the P pencils pid0 .. pid0+P-1 of the box `a`,
+// walked from end to end.  Every thread of the CTA calls it.
+template <int AXIS, int P, int T, int RING, class Policy>
+__device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0,
+                                              SweepSmem<AXIS, P, T, RING, Policy>& S) {
     using R = typename Policy::R;
     using Pow = typename Policy::Pow;
     using CT = typename Policy::CT;
     using L = SweepLayout<AXIS, P, T, RING>;
     static_assert((RING & (RING - 1)) == 0 && RING >= T + 6, "ring too small");
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy>*>(smem_raw);
 
     const int tid = threadIdx.x;
     const int tl = AXIS == 0 ? (tid % T) : (tid / P);
     const int tp = AXIS == 0 ? (tid / T) : (tid % P);
-    const long long pid = (long long)blockIdx.x * P + tp;
+    const long long pid = pid0 + tp;
     const bool active = pid < a.npencil;
     const int N = a.nsweep;
     const long long base = pencil_base<AXIS>(active ? pid : 0, a.nx, a.ny);
@@ -140,7 +150,7 @@ __global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
     const double rmax0 = dkey_decode(a.ctl->rho_key[a.bslot][1]);
     const bool peak_possible = rmax0 > k.dmax * rmin0;
 
-    if (tid == 0 && blockIdx.x == 0) {
+    if (tid == 0 && pid0 == 0) {  // once per box and sweep
         const int reset = (a.bslot + 2) % 3;
         a.ctl->rho_key[reset][0] = kKeyPosInf;
         a.ctl->rho_key[reset][1] = kKeyNegInf;
@@ -493,6 +503,68 @@ __global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
     block_flush(kmin, kmax, kvel, status, &a.ctl->rho_key[(a.bslot + 1) % 3][0],
                 &a.ctl->rho_key[(a.bslot + 1) % 3][1], (a.flags & kFlagSpeed) ? &a.ctl->velmax_key : nullptr,
                 &a.ctl->status, S.red);
+}
+
+// One box per launch: CTA b takes pencils b*P .. b*P+P-1.
+// MINB > 1 asks the compiler for at most 65536/(P*T*MINB) registers per
+// thread so that MINB CTAs fit on one SM (more warps to hide the latency of
+// the FP64 Riemann chains, at the price of spills).
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
+__global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy>*>(smem_raw);
+    sweep_pencils<AXIS, P, T, RING, Policy>(a, (long long)blockIdx.x * P, S);
+}
+
+// Many boxes per launch (the ensemble and the serving batch).  Work item i
+// is a group of P pencils of one box: entry e owns the items
+// first[e] .. first[e+1]-1 and sweeps box args[arg[e]].  A persistent grid
+// pulls items from a queue until it is empty, so boxes of different sizes
+// share the SMs without a tail per box.  All boxes of one launch are swept
+// along the same axis.
+struct BatchLaunch {
+    const SweepArgs* args;   // per (box, slot, axis) arguments
+    const int* ent;          // arg[0..nent-1], then first[0..nent]
+    int nent;
+    int nitems;              // first[nent]
+    int* counter;            // work queue head, zero before the launch
+};
+
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
+__global__ void __launch_bounds__(P* T, MINB) ppm_sweep_batch_kernel(BatchLaunch bl) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy>*>(smem_raw);
+    __shared__ SweepArgs s_args;
+    __shared__ int s_item, s_arg, s_first;
+    const int* first = bl.ent + bl.nent;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int it = atomicAdd(bl.counter, 1);
+            s_item = it;
+            if (it < bl.nitems) {
+                int lo = 0, hi = bl.nent - 1;  // last entry with first[e] <= it
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (first[mid] <= it) lo = mid;
+                    else hi = mid - 1;
+                }
+                s_arg = bl.ent[lo];
+                s_first = first[lo];
+            }
+        }
+        __syncthreads();
+        const int it = s_item;
+        if (it >= bl.nitems) break;
+        {
+            static_assert(sizeof(SweepArgs) % 8 == 0, "SweepArgs copy in 8-byte words");
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(bl.args + s_arg);
+            unsigned long long* dst = reinterpret_cast<unsigned long long*>(&s_args);
+            for (int w = threadIdx.x; w < (int)(sizeof(SweepArgs) / 8); w += blockDim.x) dst[w] = src[w];
+        }
+        __syncthreads();
+        sweep_pencils<AXIS, P, T, RING, Policy>(s_args, (long long)(it - s_first) * P, S);
+        __syncthreads();  // s_item / s_args are rewritten for the next item
+    }
 }
 
 }  // namespace hp

@@ -13,27 +13,31 @@
 
 namespace hp {
 
-constexpr int kTilesX = 8, kTilesYZ = 8;
-
-template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
-static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
+// Arguments of one sweep of box b along `axis`: the velocities permuted into
+// (normal, transverse1, transverse2) of the sweep (ppmsolver.F90:105-107,
+// 227-229, 355-357).
+static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int flags) {
     SweepArgs a;
-    // permute velocities into (normal, transverse1, transverse2) of this
-    // sweep (ppmsolver.F90:105-107, 227-229, 355-357)
     a.f[0] = b.f[0];
     a.f[1] = b.f[1];
-    if (AXIS == 0) { a.f[2] = b.f[2]; a.f[3] = b.f[3]; a.f[4] = b.f[4]; }
-    if (AXIS == 1) { a.f[2] = b.f[3]; a.f[3] = b.f[2]; a.f[4] = b.f[4]; }
-    if (AXIS == 2) { a.f[2] = b.f[4]; a.f[3] = b.f[3]; a.f[4] = b.f[2]; }
+    if (axis == 0) { a.f[2] = b.f[2]; a.f[3] = b.f[3]; a.f[4] = b.f[4]; }
+    if (axis == 1) { a.f[2] = b.f[3]; a.f[3] = b.f[2]; a.f[4] = b.f[4]; }
+    if (axis == 2) { a.f[2] = b.f[4]; a.f[3] = b.f[3]; a.f[4] = b.f[2]; }
     for (int q = 0; q < 4; ++q) a.snap[q] = b.snap[q];
     a.peak = b.peak;
     a.ctl = b.ctl;
     a.k = b.k;
     a.nx = b.nx; a.ny = b.ny; a.nz = b.nz;
-    a.nsweep = AXIS == 0 ? b.nx : (AXIS == 1 ? b.ny : b.nz);
-    a.npencil = AXIS == 0 ? (long long)b.ny * b.nz : (AXIS == 1 ? (long long)b.nx * b.nz : (long long)b.nx * b.ny);
+    a.nsweep = axis == 0 ? b.nx : (axis == 1 ? b.ny : b.nz);
+    a.npencil = axis == 0 ? (long long)b.ny * b.nz : (axis == 1 ? (long long)b.nx * b.nz : (long long)b.nx * b.ny);
     a.bslot = bslot;
     a.flags = flags;
+    return a;
+}
+
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
+static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
+    const SweepArgs a = make_sweep_args(b, AXIS, bslot, flags);
     const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy>);
     auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB>;
     static bool attr_set = false;  // per instantiation (one process drives one device)
@@ -47,42 +51,59 @@ static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
+// The tile table: (axis, tile index, P, T, RING, MINB).  The pencils per
+// CTA of each entry are also in kTilePencils (hp_launch.h); the
+// static_asserts below keep the two in step.
+#define HP_TILE_TABLE(X)                                                                       \
+    X(0, 0, 8, 32, 64, 1) X(0, 1, 4, 32, 64, 1) X(0, 2, 8, 16, 32, 1) X(0, 3, 4, 16, 32, 1)    \
+    X(0, 4, 16, 32, 64, 1) X(0, 5, 12, 32, 64, 1) X(0, 6, 8, 32, 64, 3) X(0, 7, 4, 32, 64, 5)  \
+    X(1, 0, 32, 8, 16, 1) X(1, 1, 16, 8, 16, 1) X(1, 2, 32, 4, 16, 1) X(1, 3, 16, 4, 16, 1)    \
+    X(1, 4, 64, 8, 16, 1) X(1, 5, 32, 12, 32, 1) X(1, 6, 32, 8, 16, 3) X(1, 7, 16, 8, 16, 5)   \
+    X(2, 0, 32, 8, 16, 1) X(2, 1, 16, 8, 16, 1) X(2, 2, 32, 4, 16, 1) X(2, 3, 16, 4, 16, 1)    \
+    X(2, 4, 64, 8, 16, 1) X(2, 5, 32, 12, 32, 1) X(2, 6, 32, 8, 16, 3) X(2, 7, 16, 8, 16, 5)
+
+#define HP_TILE_CHECK(AX, TI, P, T, RING, MINB) \
+    static_assert(kTilePencils[AX][TI] == P, "tile table and kTilePencils disagree");
+HP_TILE_TABLE(HP_TILE_CHECK)
+#undef HP_TILE_CHECK
+
 template <class Policy>
 static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
-    if (axis == 0) {
-        switch (tile) {
-            case 0: return launch_sweep_t<0, 8, 32, 64, Policy>(b, bslot, flags, st);
-            case 1: return launch_sweep_t<0, 4, 32, 64, Policy>(b, bslot, flags, st);
-            case 2: return launch_sweep_t<0, 8, 16, 32, Policy>(b, bslot, flags, st);
-            case 3: return launch_sweep_t<0, 4, 16, 32, Policy>(b, bslot, flags, st);
-            case 4: return launch_sweep_t<0, 16, 32, 64, Policy>(b, bslot, flags, st);
-            case 5: return launch_sweep_t<0, 12, 32, 64, Policy>(b, bslot, flags, st);
-            case 6: return launch_sweep_t<0, 8, 32, 64, Policy, 3>(b, bslot, flags, st);
-            case 7: return launch_sweep_t<0, 4, 32, 64, Policy, 5>(b, bslot, flags, st);
-        }
-    } else if (axis == 1) {
-        switch (tile) {
-            case 0: return launch_sweep_t<1, 32, 8, 16, Policy>(b, bslot, flags, st);
-            case 1: return launch_sweep_t<1, 16, 8, 16, Policy>(b, bslot, flags, st);
-            case 2: return launch_sweep_t<1, 32, 4, 16, Policy>(b, bslot, flags, st);
-            case 3: return launch_sweep_t<1, 16, 4, 16, Policy>(b, bslot, flags, st);
-            case 4: return launch_sweep_t<1, 64, 8, 16, Policy>(b, bslot, flags, st);
-            case 5: return launch_sweep_t<1, 32, 12, 32, Policy>(b, bslot, flags, st);
-            case 6: return launch_sweep_t<1, 32, 8, 16, Policy, 3>(b, bslot, flags, st);
-            case 7: return launch_sweep_t<1, 16, 8, 16, Policy, 5>(b, bslot, flags, st);
-        }
-    } else if (axis == 2) {
-        switch (tile) {
-            case 0: return launch_sweep_t<2, 32, 8, 16, Policy>(b, bslot, flags, st);
-            case 1: return launch_sweep_t<2, 16, 8, 16, Policy>(b, bslot, flags, st);
-            case 2: return launch_sweep_t<2, 32, 4, 16, Policy>(b, bslot, flags, st);
-            case 3: return launch_sweep_t<2, 16, 4, 16, Policy>(b, bslot, flags, st);
-            case 4: return launch_sweep_t<2, 64, 8, 16, Policy>(b, bslot, flags, st);
-            case 5: return launch_sweep_t<2, 32, 12, 32, Policy>(b, bslot, flags, st);
-            case 6: return launch_sweep_t<2, 32, 8, 16, Policy, 3>(b, bslot, flags, st);
-            case 7: return launch_sweep_t<2, 16, 8, 16, Policy, 5>(b, bslot, flags, st);
-        }
+#define HP_TILE_CASE(AX, TI, P, T, RING, MINB) \
+    if (axis == AX && tile == TI) return launch_sweep_t<AX, P, T, RING, Policy, MINB>(b, bslot, flags, st);
+    HP_TILE_TABLE(HP_TILE_CASE)
+#undef HP_TILE_CASE
+    return -1;
+}
+
+// Persistent batched sweep: one CTA per resident slot of the GPU (the
+// occupancy of the instantiation x the SM count), each draining the queue.
+template <int AXIS, int P, int T, int RING, class Policy, int MINB>
+static int launch_sweep_batch_t(const BatchLaunch& bl, cudaStream_t st) {
+    const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy>);
+    auto kern = ppm_sweep_batch_kernel<AXIS, P, T, RING, Policy, MINB>;
+    static int grid = 0;  // per instantiation (one process drives one device)
+    if (grid == 0) {
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return -1;
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P * T, smem) != cudaSuccess) return -1;
+        grid = sms * (per_sm > 0 ? per_sm : 1);
     }
+    const int g = bl.nitems < grid ? bl.nitems : grid;
+    if (g <= 0) return 0;
+    kern<<<g, P * T, smem, st>>>(bl);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+template <class Policy>
+static int launch_sweep_batch_policy(const BatchLaunch& bl, int axis, int tile, cudaStream_t st) {
+#define HP_TILE_CASE(AX, TI, P, T, RING, MINB) \
+    if (axis == AX && tile == TI) return launch_sweep_batch_t<AX, P, T, RING, Policy, MINB>(bl, st);
+    HP_TILE_TABLE(HP_TILE_CASE)
+#undef HP_TILE_CASE
     return -1;
 }
 

@@ -1,0 +1,123 @@
+"""Ensemble runner: many independent cosmological boxes in one batch.
+
+    python -m hydropad_b200.ensemble --boxes 64 --steps 50 --precision mixed
+
+Workload: ``--boxes`` Einstein-de Sitter Gaussian random fields, sides drawn
+from {32, 48, 64, 96, 128}, spectral index n uniform in [-2.5, -1.5], one
+seed per box (all from ``--seed``), started together at a = 1/51 and
+advanced ``--steps`` evolve_sys steps each.  The batch is autotuned, then
+timed with CUDA events on its stream; ``--alone`` also times the same boxes
+advanced one after another through hp_evolve (the one-box-per-run layout of
+the reference's main program, hydropad/main.F90:200-221).  Prints one JSON
+line (aggregate cell-updates/s).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import ics
+from .params import HydroParams
+
+SIDES = (32, 48, 64, 96, 128)
+
+
+def ensemble_specs(nboxes: int, seed: int):
+    """(side, seed, spectral index) of each box."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sides = rng.choice(SIDES, size=nboxes)
+    idx = rng.uniform(-2.5, -1.5, size=nboxes)
+    return [(int(s), int(seed * 1000 + i), float(n)) for i, (s, n) in enumerate(zip(sides, idx))]
+
+
+def make_box(side: int, seed: int, spectral_index: float, precision: str, tiles=None):
+    from .api import Hydro
+    prm = HydroParams(shape=(side, side, side), cosmo=True, tstop=(1.0 + 10.0) ** (-1.5))
+    state = ics.grf_eds(side, seed=seed, spectral_index=spectral_index)
+    h = Hydro(prm, precision=precision)
+    h.attach_state(*state)
+    if tiles is not None:
+        h.set_tiles(*tiles)
+    h.start_with_cfl()
+    return h
+
+
+def _event_ms(stream_handle: int, fn):
+    import torch
+    st = torch.cuda.ExternalStream(stream_handle)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    fn()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--boxes", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--alone", action="store_true", help="also time the boxes one after another")
+    args = ap.parse_args(argv)
+
+    from .batch import Batch
+    specs = ensemble_specs(args.boxes, args.seed)
+    cells = sum(s ** 3 for s, _, _ in specs)
+    t0 = time.perf_counter()
+    boxes = [make_box(s, sd, n, args.precision) for s, sd, n in specs]
+    t_ic = time.perf_counter() - t0
+    out = {"workload": "ensemble", "boxes": args.boxes, "sides": sorted(set(s for s, _, _ in specs)),
+           "cells": cells, "steps": args.steps, "warmup": args.warmup, "precision": args.precision,
+           "graph": not args.no_graph, "ic_seconds": round(t_ic, 2)}
+    with Batch(args.precision, capacity=args.boxes) as b:
+        for h in boxes:
+            b.add(h)
+        out["tiles"] = b.autotune(reps=1)
+        b.step(args.warmup, graph=not args.no_graph)
+        b.synchronize()
+        l0 = b.launch_count()
+        ms = _event_ms(b.stream_handle(), lambda: b.step(args.steps, graph=not args.no_graph))
+        b.synchronize()
+        out["batch_ms"] = round(ms, 3)
+        out["batch_ms_per_step"] = round(ms / args.steps, 4)
+        out["batch_cell_updates_per_s"] = cells * args.steps / (ms * 1e-3)
+        out["launches_per_step"] = (b.launch_count() - l0) / args.steps
+        tiles = out["tiles"]
+        for h in list(b.members):
+            b.remove(h)
+    for h in boxes:
+        h.close()
+    if args.alone:
+        boxes = [make_box(s, sd, n, args.precision, tiles=tiles) for s, sd, n in specs]
+        for h in boxes:
+            h.evolve(args.warmup, graph=not args.no_graph)
+
+        def run_alone():
+            for h in boxes:
+                h.evolve_async(args.steps, graph=not args.no_graph)
+
+        import torch
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run_alone()
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        out["alone_ms"] = round(ms, 3)
+        out["alone_cell_updates_per_s"] = cells * args.steps / (ms * 1e-3)
+        out["batch_speedup"] = out["batch_cell_updates_per_s"] / out["alone_cell_updates_per_s"]
+        for h in boxes:
+            h.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

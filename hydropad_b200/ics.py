@@ -84,7 +84,7 @@ def grf_eds(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float =
     with np.errstate(divide="ignore", invalid="ignore"):
         pk = np.where(k > 0, k ** spectral_index * np.exp(-(k / kc) ** 2), 0.0)
     dk = wk * np.sqrt(pk)
-    delta = np.fft.irfftn(dk, s=(n, n, n))
+    delta = np.fft.irfftn(dk, s=(n, n, n), axes=(0, 1, 2))
     norm = rms / delta.std()
     delta *= norm
     dk *= norm
@@ -97,7 +97,7 @@ def grf_eds(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float =
     vel = []
     for K in (KX, KY, KZ):
         vk = 1j * fac * dk * K * inv
-        vel.append(np.fft.irfftn(vk, s=(n, n, n)))
+        vel.append(np.fft.irfftn(vk, s=(n, n, n), axes=(0, 1, 2)))
     rho = np.maximum(1.0 + delta, rho_floor)
     tcode = temp_k / temperature_factor()
     p = rho * tcode

@@ -163,6 +163,59 @@ int hp_ppmsolver_noalloc(double *p, double *rho, double *vx, double *vy,
                          const hp_params *params, const hp_scalars *scalars,
                          void *stream);
 
+/* ---------------------------------------------------------------------
+ * Batches: many independent boxes advanced together.  No counterpart in
+ * the reference, which advances one box per run (main.F90:200-221, the
+ * time loop over evolve_sys); every member box follows exactly the
+ * reference's step (its own nrot, dt, nstep and tstop), so a box advanced
+ * in a batch is bitwise identical to the same box advanced alone by
+ * hp_evolve with the same tiles.
+ *
+ * Members are contexts created by hp_init on the batch's device with the
+ * batch's precision, with their state attached.  Each sweep of a step is
+ * one persistent launch per sweep axis over all members, pulling groups of
+ * pencils of any member from one work queue.
+ * --------------------------------------------------------------------- */
+typedef struct hp_batch hp_batch;
+
+/* capacity: the largest number of members at any time. */
+int hp_batch_create(hp_batch **out, int device, int precision, int capacity);
+/* Waits for the batch's work; the members stay valid (they are not freed). */
+int hp_batch_destroy(hp_batch *b);
+
+/* Add / remove a member between steps.  While it is a member a context is
+ * driven only by the batch: call no other hp_* function on it except
+ * hp_get_scalars / hp_download_state / hp_sync_to_host after
+ * hp_batch_synchronize.  Removing waits for the batch's pending work. */
+int hp_batch_add(hp_batch *b, hp_ctx *ctx);
+int hp_batch_remove(hp_batch *b, hp_ctx *ctx);
+int hp_batch_size(hp_batch *b);
+
+/* Enqueue nsteps evolve_sys steps of every member and return without
+ * waiting.  use_graph=1 replays one CUDA graph per nrot while every member
+ * is at the same nrot (an ensemble started together); other steps are
+ * launched directly.  Errors here are launch errors only; the members'
+ * device status is read by hp_batch_synchronize. */
+int hp_batch_step(hp_batch *b, int nsteps, int use_graph);
+
+/* Wait for the batch's work.  status[i] (if not NULL; one entry per member
+ * in the order of hp_batch_member) receives the error code of member i's
+ * device status word since the last call (then cleared); returns the first
+ * non-zero one. */
+int hp_batch_synchronize(hp_batch *b, int *status);
+hp_ctx *hp_batch_member(hp_batch *b, int i);
+
+/* Tile shape per axis of the batched sweeps (0 .. 7, as hp_set_tiles), and
+ * the autotuner over the current members (on scratch copies of their
+ * states; the states are not changed). */
+int hp_batch_set_tiles(hp_batch *b, int tile_x, int tile_y, int tile_z);
+int hp_batch_get_tiles(hp_batch *b, int *tiles /* [3] */);
+int hp_batch_autotune(hp_batch *b, int reps);
+
+/* CUDA stream of the batch (cudaStream_t) and its kernel launch count. */
+void *hp_batch_stream(hp_batch *b);
+long long hp_batch_launch_count(hp_batch *b);
+
 /* Block until the context's stream is idle and return the device status
  * word accumulated since the last call (then cleared). */
 int hp_synchronize(hp_ctx *ctx);
