@@ -91,6 +91,22 @@ class Hydro:
         self._host = arrs
         return arrs
 
+    def attach_device(self, p, rho, vx, vy, vz):
+        """Take the state from device tensors (contiguous float64, shape
+        ``(nz, ny, nx)``, x fastest, no ghosts; e.g. from
+        :func:`hydropad_b200.ics.grf_eds_device`).  The tensors are copied;
+        no host arrays are attached (use :meth:`download`)."""
+        import torch
+        shp = tuple(int(v) for v in self.params.shape)[::-1]
+        ts = (p, rho, vx, vy, vz)
+        for t in ts:
+            if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or tuple(t.shape) != shp:
+                raise ValueError(f"device state must be contiguous float64 CUDA tensors of shape {shp}")
+        torch.cuda.current_stream(ts[0].device).synchronize()
+        L.check(L.lib().hp_attach_device_state(self._ctx, *[C.c_void_p(t.data_ptr()) for t in ts]),
+                "hp_attach_device_state")
+        self._host = None
+
     def sync_to_host(self):
         L.check(L.lib().hp_sync_to_host(self._ctx), "hp_sync_to_host")
         return self._host

@@ -340,6 +340,26 @@ int hp_attach_state(hp_ctx* x, const double* p3d, const double* rho3d, const dou
     return HP_OK;
 }
 
+int hp_attach_device_state(hp_ctx* x, const double* p, const double* rho, const double* vx, const double* vy,
+                           const double* vz) {
+    if (!x || !p || !rho || !vx || !vy || !vz) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
+    const double* src[5] = {p, rho, vx, vy, vz};
+    for (int q = 0; q < 5; ++q) {
+        HP_CUDA(cudaMemcpyAsync(x->box.f[q], src[q], n * sizeof(double), cudaMemcpyDeviceToDevice, x->stream));
+        x->host[q] = nullptr;
+    }
+    x->hnx = x->box.nx; x->hny = x->box.ny; x->hnz = x->box.nz; x->hnb = 0;
+    x->attached = true;
+    x->sweep_count = 0;
+    const int nk = hp::launch_bounds(x->box, 0, x->stream);
+    if (nk < 0) return HP_ERR_CUDA;
+    x->launches += nk;
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return HP_OK;
+}
+
 int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, double* vy3d, double* vz3d, int nx,
                       int ny, int nz, int nbound) {
     if (!x || !p3d || !rho3d || !vx3d || !vy3d || !vz3d) return HP_ERR_ARG;
@@ -359,7 +379,7 @@ int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, doubl
 
 int hp_sync_to_host(hp_ctx* x) {
     if (!x) return HP_ERR_ARG;
-    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    if (!x->attached || !x->host[0]) return HP_ERR_NOT_ATTACHED;  // no host arrays behind a device attach
     return hp_download_state(x, (double*)x->host[0], (double*)x->host[1], (double*)x->host[2], (double*)x->host[3],
                              (double*)x->host[4], x->hnx, x->hny, x->hnz, x->hnb);
 }

@@ -6,8 +6,10 @@
 * :func:`grf_eds` -- a seeded Gaussian random baryon field on an EdS
   background with linear-theory velocities and uniform temperature (the
   cosmological configurations; reference analogue initvel.F90:31-37).
+* :func:`grf_eds_device` -- the same field with the FFT work on the GPU,
+  returned as device tensors (serving and large boxes).
 
-Every function returns ``(p, rho, vx, vy, vz)`` as ghosted Fortran-order
+The host functions return ``(p, rho, vx, vy, vz)`` as ghosted Fortran-order
 float64 arrays ``(N+2nb, ...)`` with periodic ghosts filled.
 """
 from __future__ import annotations
@@ -102,3 +104,51 @@ def grf_eds(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float =
     tcode = temp_k / temperature_factor()
     p = rho * tcode
     return tuple(_ghost(np.ascontiguousarray(a), nb) for a in (p, rho, vel[0], vel[1], vel[2]))
+
+
+def grf_eds_device(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float = 0.5,
+                   spectral_index: float = -2.0, kc_frac: float = 1.0 / 8.0, temp_k: float = 100.0,
+                   rho_floor: float = 1e-2, device="cuda"):
+    """:func:`grf_eds` with the spectral work on the GPU.
+
+    The white noise is the same PCG64 draw as :func:`grf_eds` (generated on
+    the host, so a seed gives the same field on every path); the FFTs, the
+    power-spectrum filter and the linear velocities run on ``device`` in
+    FP64.  Returns ``(p, rho, vx, vy, vz)`` as contiguous float64 device
+    tensors in the device state layout: shape ``(n, n, n)`` indexed
+    ``[z, y, x]`` (x fastest), no ghosts -- the input of
+    ``Hydro.attach_device``.  Agrees with :func:`grf_eds` to FFT rounding."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    white = torch.from_numpy(rng.standard_normal((n, n, n))).to(device)  # indexed [x, y, z] like grf_eds
+    wk = torch.fft.rfftn(white)
+    del white
+    f64 = dict(dtype=torch.float64, device=wk.device)
+    kx = torch.fft.fftfreq(n, **f64) * n
+    kz = torch.fft.rfftfreq(n, **f64) * n
+    KX, KY, KZ = kx[:, None, None], kx[None, :, None], kz[None, None, :]
+    k2 = KX * KX + KY * KY + KZ * KZ
+    k = torch.sqrt(k2)
+    kc = kc_frac * n
+    pk = torch.where(k > 0, k.pow(spectral_index) * torch.exp(-(k / kc) ** 2), torch.zeros_like(k))
+    dk = wk * torch.sqrt(pk)
+    del wk, pk, k
+    delta = torch.fft.irfftn(dk, s=(n, n, n))
+    norm = rms / float(delta.std(correction=0))
+    delta *= norm
+    dk *= norm
+    tin, at, dat = eds_time(a_start)
+    fac = at * (dat / at)  # a H f, f = 1
+    two_pi = 2.0 * np.pi
+    inv = torch.where(k2 > 0, 1.0 / (two_pi * k2), torch.zeros_like(k2))
+    del k2
+    to_dev = lambda a: a.permute(2, 1, 0).contiguous()  # [x, y, z] -> memory x fastest
+    vel = []
+    for K in (KX, KY, KZ):
+        vk = (1j * fac) * dk * (K * inv)
+        vel.append(to_dev(torch.fft.irfftn(vk, s=(n, n, n))))
+        del vk
+    rho = torch.clamp(1.0 + delta, min=rho_floor)
+    tcode = temp_k / temperature_factor()
+    p = rho * tcode
+    return to_dev(p), to_dev(rho), vel[0], vel[1], vel[2]

@@ -95,6 +95,16 @@ int hp_attach_state(hp_ctx *ctx, const double *p3d, const double *rho3d,
                     const double *vx3d, const double *vy3d, const double *vz3d,
                     const double *gforce, int nx, int ny, int nz, int nbound);
 
+/* Take the state from DEVICE arrays on the context's device (dense
+ * (ngridx,ngridy,ngridz) interiors, x fastest; copied, the caller keeps
+ * them), e.g. initial conditions generated on the GPU.  The caller's writes
+ * must be complete (synchronise the producing stream first).  No host
+ * arrays are attached: hp_sync_to_host and hp_ppmsolver then report
+ * HP_ERR_NOT_ATTACHED / HP_ERR_STATE_MISMATCH; use hp_download_state.
+ * No counterpart in the reference, whose state is born on the host. */
+int hp_attach_device_state(hp_ctx *ctx, const double *p, const double *rho,
+                           const double *vx, const double *vy, const double *vz);
+
 /* Download the resident state into the attached host arrays (interior) and
  * refill their periodic ghost layers. */
 int hp_sync_to_host(hp_ctx *ctx);
