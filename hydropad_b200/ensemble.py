@@ -10,6 +10,10 @@ timed with CUDA events on its stream; ``--alone`` also times the same boxes
 advanced one after another through hp_evolve (the one-box-per-run layout of
 the reference's main program, hydropad/main.F90:200-221).  Prints one JSON
 line (aggregate cell-updates/s).
+
+Under torchrun (one process per GPU) the boxes are split across the ranks by
+:func:`hydropad_b200.shard.assign_lpt` (cells per box); each rank times its
+own batch on its device and the job's time is the maximum over the ranks.
 """
 from __future__ import annotations
 
@@ -26,19 +30,19 @@ SIDES = (32, 48, 64, 96, 128)
 
 
 def ensemble_specs(nboxes: int, seed: int):
-    """(side, seed, spectral index) of each box."""
+    """(side, seed, spectral index) of each box: box i has seed i; sides and
+    spectral indices are drawn from ``seed``."""
     rng = np.random.Generator(np.random.PCG64(seed))
     sides = rng.choice(SIDES, size=nboxes)
     idx = rng.uniform(-2.5, -1.5, size=nboxes)
-    return [(int(s), int(seed * 1000 + i), float(n)) for i, (s, n) in enumerate(zip(sides, idx))]
+    return [(int(s), i, float(n)) for i, (s, n) in enumerate(zip(sides, idx))]
 
 
-def make_box(side: int, seed: int, spectral_index: float, precision: str, tiles=None):
+def make_box(side: int, seed: int, spectral_index: float, precision: str, tiles=None, device: int = 0):
     from .api import Hydro
     prm = HydroParams(shape=(side, side, side), cosmo=True, tstop=(1.0 + 10.0) ** (-1.5))
-    state = ics.grf_eds(side, seed=seed, spectral_index=spectral_index)
-    h = Hydro(prm, precision=precision)
-    h.attach_state(*state)
+    h = Hydro(prm, precision=precision, device=device)
+    h.attach_device(*ics.grf_eds_device(side, seed=seed, spectral_index=spectral_index, device=f"cuda:{device}"))
     if tiles is not None:
         h.set_tiles(*tiles)
     h.start_with_cfl()
@@ -69,34 +73,56 @@ def main(argv=None):
     ap.add_argument("--alone", action="store_true", help="also time the boxes one after another")
     args = ap.parse_args(argv)
 
+    import os
+
+    import torch
+
     from .batch import Batch
+    from .shard import assign_lpt, gather_objects
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(dev)
     specs = ensemble_specs(args.boxes, args.seed)
     cells = sum(s ** 3 for s, _, _ in specs)
+    mine = [specs[i] for i in assign_lpt([s ** 3 for s, _, _ in specs], world)[rank]]
+    my_cells = sum(s ** 3 for s, _, _ in mine)
     t0 = time.perf_counter()
-    boxes = [make_box(s, sd, n, args.precision) for s, sd, n in specs]
+    boxes = [make_box(s, sd, n, args.precision, device=dev) for s, sd, n in mine]
     t_ic = time.perf_counter() - t0
     out = {"workload": "ensemble", "boxes": args.boxes, "sides": sorted(set(s for s, _, _ in specs)),
            "cells": cells, "steps": args.steps, "warmup": args.warmup, "precision": args.precision,
-           "graph": not args.no_graph, "ic_seconds": round(t_ic, 2)}
-    with Batch(args.precision, capacity=args.boxes) as b:
+           "graph": not args.no_graph, "ic_seconds": round(t_ic, 2), "n_gpus": world}
+    with Batch(args.precision, capacity=max(1, len(mine)), device=dev) as b:
         for h in boxes:
             b.add(h)
-        out["tiles"] = b.autotune(reps=1)
+        tiles = b.autotune(reps=1)
         b.step(args.warmup, graph=not args.no_graph)
         b.synchronize()
+        gather_objects(None)  # barrier
         l0 = b.launch_count()
         ms = _event_ms(b.stream_handle(), lambda: b.step(args.steps, graph=not args.no_graph))
         b.synchronize()
-        out["batch_ms"] = round(ms, 3)
-        out["batch_ms_per_step"] = round(ms / args.steps, 4)
-        out["batch_cell_updates_per_s"] = cells * args.steps / (ms * 1e-3)
-        out["launches_per_step"] = (b.launch_count() - l0) / args.steps
-        tiles = out["tiles"]
+        per_rank = gather_objects({"ms": ms, "cells": my_cells, "boxes": len(mine), "tiles": list(tiles),
+                                   "launches": (b.launch_count() - l0) / args.steps})
         for h in list(b.members):
             b.remove(h)
     for h in boxes:
         h.close()
-    if args.alone:
+    ms = max(r["ms"] for r in per_rank)
+    out["tiles"] = tiles
+    out["batch_ms"] = round(ms, 3)
+    out["batch_ms_per_step"] = round(ms / args.steps, 4)
+    out["batch_cell_updates_per_s"] = cells * args.steps / (ms * 1e-3)
+    out["launches_per_step"] = per_rank[0]["launches"]
+    if world > 1:
+        out["per_rank"] = per_rank
+    if args.alone and world == 1:
         boxes = [make_box(s, sd, n, args.precision, tiles=tiles) for s, sd, n in specs]
         for h in boxes:
             h.evolve(args.warmup, graph=not args.no_graph)
@@ -105,7 +131,6 @@ def main(argv=None):
             for h in boxes:
                 h.evolve_async(args.steps, graph=not args.no_graph)
 
-        import torch
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         run_alone()
@@ -116,7 +141,11 @@ def main(argv=None):
         out["batch_speedup"] = out["batch_cell_updates_per_s"] / out["alone_cell_updates_per_s"]
         for h in boxes:
             h.close()
-    print(json.dumps(out))
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -127,6 +127,22 @@ class ServeStats:
         }
 
 
+def merge_stats(parts) -> ServeStats:
+    """One job's statistics from the per-rank ones (each rank serves its own
+    share of the trace on its own GPU)."""
+    out = ServeStats()
+    for st in parts:
+        out.completed.extend(st.completed)
+        out.admission_stalls += st.admission_stalls
+        out.stall_seconds += st.stall_seconds
+        out.max_queue = max(out.max_queue, st.max_queue)
+        out.peak_resident_bytes = max(out.peak_resident_bytes, st.peak_resident_bytes)
+        out.steps_launched += st.steps_launched
+        out.wall = max(out.wall, st.wall)
+    out.completed.sort(key=lambda c: c.rid)
+    return out
+
+
 class Scheduler:
     """Continuous batching at step boundaries under an HBM budget.
 
@@ -338,19 +354,42 @@ def main(argv=None):
     ap.add_argument("--pool-gb", type=float, default=0.0, help="keep finished contexts for reuse up to this size")
     args = ap.parse_args(argv)
 
+    import os
+
     import torch
+
+    from .shard import gather_objects, shard_trace
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
+    torch.cuda.set_device(dev)
     trace = poisson_trace(args.requests, rate=args.rate, seed=args.trace_seed)
+    mine = shard_trace(trace, world)[rank]
     free, _total = torch.cuda.mem_get_info()
     budget = int(args.budget_gb * 1e9) if args.budget_gb > 0 else int(0.8 * free)
-    tiles = tune_tiles(args.precision) if args.tiles == "auto" else tuple(int(t) for t in args.tiles.split(","))
-    eng = GpuEngine(args.precision, capacity=args.capacity, tiles=tiles, pool_bytes=int(args.pool_gb * 1e9))
+    tiles = (tune_tiles(args.precision, device=dev) if args.tiles == "auto"
+             else tuple(int(t) for t in args.tiles.split(",")))
+    eng = GpuEngine(args.precision, capacity=args.capacity, tiles=tiles, device=dev,
+                    pool_bytes=int(args.pool_gb * 1e9))
     try:
         sched = Scheduler(eng, budget - eng.pool_bytes, capacity=args.capacity, chunk=args.chunk)
+        gather_objects(None)  # barrier: the ranks start the trace clock together
         eng.start_clock()
-        st = sched.run(trace)
+        st = sched.run(mine)
     finally:
         eng.close()
-    out = {"workload": "serving", "precision": args.precision, "rate_per_s": args.rate,
+    st = merge_stats(gather_objects(st))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {"workload": "serving", "precision": args.precision, "rate_per_s": args.rate, "n_gpus": world,
            "trace_seed": args.trace_seed, "budget_gb": budget / 1e9, "capacity": args.capacity,
            "chunk": args.chunk, "tiles": list(tiles), "pool_gb": args.pool_gb,
            "offered_cell_updates_per_s": args.rate * float(np.mean([r.cells * r.steps for r in trace]))}
