@@ -7,7 +7,11 @@ Einstein-de Sitter background from z=50, seeded Gaussian random baryon field
 T = 100 K.  One step = one evolve_sys hydro step: three fused directional
 sweeps, expand, CFL reduction and timedet, all on the device.  The headline
 value is the mixed-precision path; the FP64 path is measured beside it and
-the density relative L1 between the two is reported.
+the density relative L1 between the two is reported.  Beside the headline:
+the batched ensemble (64 boxes of 32^3..128^3, mixed, 50 steps, one
+persistent launch per sweep axis, CUDA graphs) and a bounded serving trace
+(Poisson arrivals at 200/s, sides 32..256, 50..500 steps; p50/p99 latency from
+arrival to result on the host, aggregate cell-updates/s), mixed and FP64.
 
     python bench.py [--steps K] [--warmup W] [--n 256]
     torchrun --nproc-per-node N bench.py --gpus N      # one box per GPU (weak)
@@ -43,6 +47,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--serve-requests", type=int, default=32,
+                    help="requests of the serving trace (0: skip the serving and ensemble runs)")
     return ap.parse_args()
 
 
@@ -232,6 +238,29 @@ def run_ours(args):
                "path": "hp_attach_state + hp_evolve(1) + hp_sync_to_host, pinned ghosted Fortran arrays"}
         h.close()
 
+    # the batched paths: the 64-box ensemble (mixed, 50 steps) and a bounded
+    # serving trace (Poisson arrivals at 200/s), both split across the ranks
+    ensemble = serving = None
+    if args.serve_requests > 0:
+        from hydropad_b200.ensemble import run_ensemble
+        from hydropad_b200.serve import run_serving
+        from hydropad_b200.shard import gather_objects
+        per_rank = gather_objects(run_ensemble(64, 50, 3, "mixed", 4, True, world, rank, local))
+        ems = max(r["ms"] for r in per_rank)
+        ensemble = {"boxes": 64, "sides": per_rank[0]["sides"], "cells": per_rank[0]["total_cells"], "steps": 50,
+                    "precision": "mixed", "tiles": per_rank[0]["tiles"], "ms_per_step": ems / 50,
+                    "value": per_rank[0]["total_cells"] * 50 / (ems * 1e-3), "unit": UNIT,
+                    "launches_per_step": per_rank[0]["launches"] / 50}
+        serving = {"requests": args.serve_requests, "rate_per_s": 200.0, "trace_seed": 2024}
+        for prec in ("mixed", "fp64"):
+            st, stiles = run_serving(args.serve_requests, 200.0, 2024, prec, world=world, rank=rank, device=local)
+            sm = st.summary()
+            serving[prec] = {"p50_s": sm["latency_p50_s"], "p99_s": sm["latency_p99_s"],
+                             "value": sm["cell_updates_per_s"], "unit": UNIT, "makespan_s": sm["makespan_s"],
+                             "admission_stalls": sm["admission_stalls"], "tiles": list(stiles)}
+        serving["offered_cell_updates_per_s"] = st.offered
+        serving["budget_gb_per_gpu"] = st.budget_bytes / 1e9
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(state, prm, args)
@@ -275,6 +304,8 @@ def run_ours(args):
         "clocks": mx["clocks"],
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "ensemble": ensemble,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
 

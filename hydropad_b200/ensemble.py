@@ -62,6 +62,38 @@ def _event_ms(stream_handle: int, fn):
     return e0.elapsed_time(e1)
 
 
+def run_ensemble(boxes: int = 64, steps: int = 50, warmup: int = 3, precision: str = "mixed", seed: int = 4,
+                 graph: bool = True, world: int = 1, rank: int = 0, device: int = 0) -> dict:
+    """This rank's share of the ensemble (LPT split by cells), autotuned and
+    timed with CUDA events on the batch's stream.  Returns the rank's
+    figures; the caller takes the maximum time over the ranks."""
+    from .batch import Batch
+    from .shard import assign_lpt, gather_objects
+    specs = ensemble_specs(boxes, seed)
+    mine = [specs[i] for i in assign_lpt([s ** 3 for s, _, _ in specs], world)[rank]]
+    t0 = time.perf_counter()
+    hs = [make_box(s, sd, n, precision, device=device) for s, sd, n in mine]
+    t_ic = time.perf_counter() - t0
+    with Batch(precision, capacity=max(1, len(mine)), device=device) as b:
+        for h in hs:
+            b.add(h)
+        tiles = b.autotune(reps=1)
+        b.step(warmup, graph=graph)
+        b.synchronize()
+        gather_objects(None)  # barrier
+        l0 = b.launch_count()
+        ms = _event_ms(b.stream_handle(), lambda: b.step(steps, graph=graph))
+        b.synchronize()
+        launches = b.launch_count() - l0
+        for h in list(b.members):
+            b.remove(h)
+    for h in hs:
+        h.close()
+    return {"ms": ms, "cells": sum(s ** 3 for s, _, _ in mine), "boxes": len(mine), "tiles": list(tiles),
+            "launches": launches, "ic_seconds": t_ic, "total_cells": sum(s ** 3 for s, _, _ in specs),
+            "sides": sorted(set(s for s, _, _ in specs))}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--boxes", type=int, default=64)
@@ -77,8 +109,7 @@ def main(argv=None):
 
     import torch
 
-    from .batch import Batch
-    from .shard import assign_lpt, gather_objects
+    from .shard import gather_objects
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -88,52 +119,28 @@ def main(argv=None):
         import torch.distributed as dist
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(dev)
-    specs = ensemble_specs(args.boxes, args.seed)
-    cells = sum(s ** 3 for s, _, _ in specs)
-    mine = [specs[i] for i in assign_lpt([s ** 3 for s, _, _ in specs], world)[rank]]
-    my_cells = sum(s ** 3 for s, _, _ in mine)
-    t0 = time.perf_counter()
-    boxes = [make_box(s, sd, n, args.precision, device=dev) for s, sd, n in mine]
-    t_ic = time.perf_counter() - t0
-    out = {"workload": "ensemble", "boxes": args.boxes, "sides": sorted(set(s for s, _, _ in specs)),
-           "cells": cells, "steps": args.steps, "warmup": args.warmup, "precision": args.precision,
-           "graph": not args.no_graph, "ic_seconds": round(t_ic, 2), "n_gpus": world}
-    with Batch(args.precision, capacity=max(1, len(mine)), device=dev) as b:
-        for h in boxes:
-            b.add(h)
-        tiles = b.autotune(reps=1)
-        b.step(args.warmup, graph=not args.no_graph)
-        b.synchronize()
-        gather_objects(None)  # barrier
-        l0 = b.launch_count()
-        ms = _event_ms(b.stream_handle(), lambda: b.step(args.steps, graph=not args.no_graph))
-        b.synchronize()
-        per_rank = gather_objects({"ms": ms, "cells": my_cells, "boxes": len(mine), "tiles": list(tiles),
-                                   "launches": (b.launch_count() - l0) / args.steps})
-        for h in list(b.members):
-            b.remove(h)
-    for h in boxes:
-        h.close()
+    mine = run_ensemble(args.boxes, args.steps, args.warmup, args.precision, args.seed, not args.no_graph,
+                        world, rank, dev)
+    per_rank = gather_objects(mine)
     ms = max(r["ms"] for r in per_rank)
-    out["tiles"] = tiles
-    out["batch_ms"] = round(ms, 3)
-    out["batch_ms_per_step"] = round(ms / args.steps, 4)
-    out["batch_cell_updates_per_s"] = cells * args.steps / (ms * 1e-3)
-    out["launches_per_step"] = per_rank[0]["launches"]
+    cells = mine["total_cells"]
+    tiles = mine["tiles"]
+    out = {"workload": "ensemble", "boxes": args.boxes, "sides": mine["sides"], "cells": cells,
+           "steps": args.steps, "warmup": args.warmup, "precision": args.precision, "graph": not args.no_graph,
+           "n_gpus": world, "tiles": tiles, "batch_ms": round(ms, 3), "batch_ms_per_step": round(ms / args.steps, 4),
+           "batch_cell_updates_per_s": cells * args.steps / (ms * 1e-3),
+           "launches_per_step": per_rank[0]["launches"] / args.steps}
     if world > 1:
         out["per_rank"] = per_rank
     if args.alone and world == 1:
+        specs = ensemble_specs(args.boxes, args.seed)
         boxes = [make_box(s, sd, n, args.precision, tiles=tiles) for s, sd, n in specs]
         for h in boxes:
             h.evolve(args.warmup, graph=not args.no_graph)
-
-        def run_alone():
-            for h in boxes:
-                h.evolve_async(args.steps, graph=not args.no_graph)
-
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        run_alone()
+        for h in boxes:
+            h.evolve_async(args.steps, graph=not args.no_graph)
         torch.cuda.synchronize()
         ms = (time.perf_counter() - t0) * 1e3
         out["alone_ms"] = round(ms, 3)

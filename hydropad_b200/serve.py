@@ -105,6 +105,8 @@ class ServeStats:
     peak_resident_bytes: int = 0
     steps_launched: int = 0
     wall: float = 0.0
+    budget_bytes: int = 0              # HBM budget of one rank
+    offered: float = 0.0               # offered load of the whole trace, cell-updates/s
 
     def summary(self) -> dict:
         lat = np.array([c.latency for c in self.completed]) if self.completed else np.zeros(1)
@@ -340,6 +342,35 @@ def run_alone(req: Request, precision: str, tiles=None, device: int = 0):
         return h.download(nbound=0)
 
 
+def run_serving(requests: int = 100, rate: float = 200.0, trace_seed: int = 2024, precision: str = "mixed",
+                budget_bytes: int = 0, capacity: int = 64, chunk: int = 8, tiles=None, pool_bytes: int = 0,
+                world: int = 1, rank: int = 0, device: int = 0):
+    """This rank's share of the serving trace (:func:`shard_trace`), then one
+    host gather: returns (merged statistics of every rank, tiles)."""
+    import torch
+
+    from .shard import gather_objects, shard_trace
+    trace = poisson_trace(requests, rate=rate, seed=trace_seed)
+    mine = shard_trace(trace, world)[rank]
+    if budget_bytes <= 0:
+        free, _total = torch.cuda.mem_get_info(device)
+        budget_bytes = int(0.8 * free)
+    if tiles is None:
+        tiles = tune_tiles(precision, device=device)
+    eng = GpuEngine(precision, capacity=capacity, tiles=tiles, device=device, pool_bytes=pool_bytes)
+    try:
+        sched = Scheduler(eng, budget_bytes - eng.pool_bytes, capacity=capacity, chunk=chunk)
+        gather_objects(None)  # barrier: the ranks start the trace clock together
+        eng.start_clock()
+        st = sched.run(mine)
+    finally:
+        eng.close()
+    st = merge_stats(gather_objects(st))
+    st.budget_bytes = budget_bytes
+    st.offered = rate * float(np.mean([r.cells * r.steps for r in trace]))
+    return st, tuple(tiles)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=100)
@@ -357,8 +388,6 @@ def main(argv=None):
     import os
 
     import torch
-
-    from .shard import gather_objects, shard_trace
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -368,31 +397,18 @@ def main(argv=None):
         import torch.distributed as dist
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
     torch.cuda.set_device(dev)
-    trace = poisson_trace(args.requests, rate=args.rate, seed=args.trace_seed)
-    mine = shard_trace(trace, world)[rank]
-    free, _total = torch.cuda.mem_get_info()
-    budget = int(args.budget_gb * 1e9) if args.budget_gb > 0 else int(0.8 * free)
-    tiles = (tune_tiles(args.precision, device=dev) if args.tiles == "auto"
-             else tuple(int(t) for t in args.tiles.split(",")))
-    eng = GpuEngine(args.precision, capacity=args.capacity, tiles=tiles, device=dev,
-                    pool_bytes=int(args.pool_gb * 1e9))
-    try:
-        sched = Scheduler(eng, budget - eng.pool_bytes, capacity=args.capacity, chunk=args.chunk)
-        gather_objects(None)  # barrier: the ranks start the trace clock together
-        eng.start_clock()
-        st = sched.run(mine)
-    finally:
-        eng.close()
-    st = merge_stats(gather_objects(st))
+    tiles = None if args.tiles == "auto" else tuple(int(t) for t in args.tiles.split(","))
+    st, tiles = run_serving(args.requests, args.rate, args.trace_seed, args.precision, int(args.budget_gb * 1e9),
+                            args.capacity, args.chunk, tiles, int(args.pool_gb * 1e9), world, rank, dev)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     if rank != 0:
         return
     out = {"workload": "serving", "precision": args.precision, "rate_per_s": args.rate, "n_gpus": world,
-           "trace_seed": args.trace_seed, "budget_gb": budget / 1e9, "capacity": args.capacity,
+           "trace_seed": args.trace_seed, "budget_gb": st.budget_bytes / 1e9, "capacity": args.capacity,
            "chunk": args.chunk, "tiles": list(tiles), "pool_gb": args.pool_gb,
-           "offered_cell_updates_per_s": args.rate * float(np.mean([r.cells * r.steps for r in trace]))}
+           "offered_cell_updates_per_s": st.offered}
     out.update(st.summary())
     print(json.dumps(out))
 
