@@ -107,6 +107,12 @@ class Hydro:
                 "hp_attach_device_state")
         self._host = None
 
+    def write_var(self, directory: str, fp64: bool = False):
+        """The reference's end-of-run dump (write_var_mpi): rho.bin,
+        pressure.bin, vx.bin, vy.bin, vz.bin, raw REAL(4) interiors in
+        Fortran order (``fp64=True``: REAL(8) to ``*.f64.bin``)."""
+        L.check(L.lib().hp_write_var(self._ctx, str(directory).encode(), 1 if fp64 else 0), "hp_write_var")
+
     def sync_to_host(self):
         L.check(L.lib().hp_sync_to_host(self._ctx), "hp_sync_to_host")
         return self._host
@@ -156,9 +162,9 @@ class Hydro:
         L.check(L.lib().hp_evolve(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve")
 
     def evolve_async(self, nsteps: int, graph: bool = True):
-        """Enqueue nsteps without the final status read (for timing loops);
-        call :meth:`synchronize` afterwards."""
-        L.check(L.lib().hp_evolve(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve")
+        """Enqueue nsteps without waiting or reading the status (for timing
+        loops); call :meth:`synchronize` afterwards."""
+        L.check(L.lib().hp_evolve_async(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve_async")
 
     def synchronize(self):
         L.check(L.lib().hp_synchronize(self._ctx), "hp_synchronize")

@@ -377,6 +377,71 @@ int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, doubl
     return HP_OK;
 }
 
+int hp_write_var(hp_ctx* x, const char* directory, int fp64) {
+    if (!x || !directory) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    HP_CUDA(cudaSetDevice(x->dev));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    // main.F90:125-135 order and names; field index in box.f (p, rho, vx, vy, vz)
+    static const char* kNames[5] = {"rho", "pressure", "vx", "vy", "vz"};
+    static const int kField[5] = {1, 0, 2, 3, 4};
+    const long long n = (long long)x->box.nx * x->box.ny * x->box.nz;
+    const size_t esize = fp64 ? sizeof(double) : sizeof(float);
+    // the FP32 copy is staged in the density-peak buffer (n doubles), which
+    // holds nothing between steps
+    float* f32 = reinterpret_cast<float*>(x->box.peak);
+    constexpr size_t kChunk = 64u << 20;  // bytes per pinned staging buffer
+    unsigned char* pin[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    int rc = HP_OK;
+    for (int b = 0; b < 2 && rc == HP_OK; ++b) {
+        rc = cuda_fail(cudaMallocHost(&pin[b], kChunk));
+        if (rc == HP_OK) rc = cuda_fail(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+    }
+    for (int v = 0; v < 5 && rc == HP_OK; ++v) {
+        const unsigned char* src;
+        if (fp64) {
+            src = reinterpret_cast<const unsigned char*>(x->box.f[kField[v]]);
+        } else {
+            if (hp::launch_to_f32(x->box.f[kField[v]], f32, n, x->stream) < 0) { rc = HP_ERR_CUDA; break; }
+            x->launches += 1;
+            src = reinterpret_cast<const unsigned char*>(f32);
+        }
+        char path[4096];
+        snprintf(path, sizeof path, "%s/%s%s.bin", directory, kNames[v], fp64 ? ".f64" : "");
+        FILE* fp = fopen(path, "wb");
+        if (!fp) { rc = HP_ERR_ARG; break; }
+        // double-buffered: copy chunk c+1 while chunk c is written
+        const size_t total = (size_t)n * esize;
+        size_t off = 0, pending = 0;
+        int cur = 0;
+        while (rc == HP_OK && (off < total || pending)) {
+            size_t len = 0;
+            if (off < total) {
+                len = total - off < kChunk ? total - off : kChunk;
+                rc = cuda_fail(cudaMemcpyAsync(pin[cur], src + off, len, cudaMemcpyDeviceToHost, x->stream));
+                if (rc == HP_OK) rc = cuda_fail(cudaEventRecord(ev[cur], x->stream));
+            }
+            if (rc == HP_OK && pending) {
+                const int prev = cur ^ 1;
+                rc = cuda_fail(cudaEventSynchronize(ev[prev]));
+                if (rc == HP_OK && fwrite(pin[prev], 1, pending, fp) != pending) rc = HP_ERR_ARG;
+            }
+            off += len;
+            pending = len;
+            cur ^= 1;
+            if (len == 0) break;
+        }
+        if (fclose(fp) != 0 && rc == HP_OK) rc = HP_ERR_ARG;
+    }
+    cudaStreamSynchronize(x->stream);
+    for (int b = 0; b < 2; ++b) {
+        if (pin[b]) cudaFreeHost(pin[b]);
+        if (ev[b]) cudaEventDestroy(ev[b]);
+    }
+    return rc;
+}
+
 int hp_sync_to_host(hp_ctx* x) {
     if (!x) return HP_ERR_ARG;
     if (!x->attached || !x->host[0]) return HP_ERR_NOT_ATTACHED;  // no host arrays behind a device attach
@@ -438,7 +503,7 @@ int hp_timedet(hp_ctx* x, double velmax) {
     return HP_OK;
 }
 
-int hp_evolve(hp_ctx* x, int nsteps, int use_graph) {
+int hp_evolve_async(hp_ctx* x, int nsteps, int use_graph) {
     if (!x || nsteps < 0) return HP_ERR_ARG;
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     HP_CUDA(cudaSetDevice(x->dev));
@@ -471,6 +536,12 @@ int hp_evolve(hp_ctx* x, int nsteps, int use_graph) {
         }
         x->nstep_host += 1;
     }
+    return HP_OK;
+}
+
+int hp_evolve(hp_ctx* x, int nsteps, int use_graph) {
+    const int rc = hp_evolve_async(x, nsteps, use_graph);
+    if (rc != HP_OK) return rc;
     return hp_synchronize(x);
 }
 

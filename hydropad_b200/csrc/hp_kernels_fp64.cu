@@ -150,6 +150,18 @@ int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st) {
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
+// FP64 -> FP32, round to nearest even (Fortran REAL() of a REAL(8), the
+// conversion write_var_mpi.F90:55 applies before writing).
+__global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = __double2float_rn(in[i]);
+}
+
+int launch_to_f32(const double* in, float* out, long long n, cudaStream_t st) {
+    to_f32_kernel<<<592, 256, 0, st>>>(in, out, n);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
 // Status words of a batch's boxes into out[], each cleared.
 __global__ void status_gather_kernel(DevCtl* const* __restrict__ ctls, int n, unsigned* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -39,6 +39,8 @@ int launch_sweep_batch(const BatchLaunch& bl, int axis, int tile, int precision,
 int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st);
 // timedet (advance = 1) on n control blocks.
 int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st);
+// out[i] = (float)in[i], round to nearest even.
+int launch_to_f32(const double* in, float* out, long long n, cudaStream_t st);
 // out[i] = status word of ctls[i], which is cleared.
 int launch_status_gather(DevCtl* const* ctls, int n, unsigned* out, cudaStream_t st);
 

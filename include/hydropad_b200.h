@@ -109,6 +109,15 @@ int hp_attach_device_state(hp_ctx *ctx, const double *p, const double *rho,
  * refill their periodic ghost layers. */
 int hp_sync_to_host(hp_ctx *ctx);
 
+/* The end-of-run dump of main.F90:125-135 (write_var_mpi, io/write_var_mpi.F90:
+ * 1-65): rho.bin, pressure.bin, vx.bin, vy.bin, vz.bin in `directory`, each
+ * the interior (ngridx,ngridy,ngridz) in Fortran order as raw native
+ * (little-endian) REAL(4), no header, converted on the device with
+ * round-to-nearest.  fp64=1 writes the same layout in REAL(8) to
+ * rho.f64.bin, pressure.f64.bin, ... (no counterpart in the reference).
+ * Existing files are replaced.  Uses the density-peak buffer as staging. */
+int hp_write_var(hp_ctx *ctx, const char *directory, int fp64);
+
 /* Download into arbitrary host arrays of the same shape. */
 int hp_download_state(hp_ctx *ctx, double *p3d, double *rho3d, double *vx3d,
                       double *vy3d, double *vz3d, int nx, int ny, int nz,
@@ -141,6 +150,9 @@ int hp_timedet(hp_ctx *ctx, double velmax);
  * use_graph=1 captures one step per nrot value in CUDA graphs and replays
  * them.  Returns the accumulated error status. */
 int hp_evolve(hp_ctx *ctx, int nsteps, int use_graph);
+/* hp_evolve without the final wait and status read: returns once the steps
+ * are enqueued on the context's stream (hp_synchronize reads the status). */
+int hp_evolve_async(hp_ctx *ctx, int nsteps, int use_graph);
 
 /* Sweep tile shape per axis (0 .. 7; pencils per CTA x cells per window
  * step).  Results do not depend on the tile, only the speed does.  No
