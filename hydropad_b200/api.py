@@ -60,6 +60,7 @@ class Hydro:
         self._ctx = C.c_void_p()
         L.check(L.lib().hp_init(C.byref(p), C.byref(self._ctx)), "hp_init")
         self._host = None
+        self._gforce = None
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -80,15 +81,23 @@ class Hydro:
         self.close()
 
     # -- state --------------------------------------------------------------
-    def attach_state(self, p3d, rho3d, vx3d, vy3d, vz3d):
+    def attach_state(self, p3d, rho3d, vx3d, vy3d, vz3d, gforce=None):
         """Upload ghosted Fortran-order host arrays; the device copy becomes
-        the working state (the arrays are kept for :meth:`sync_to_host`)."""
+        the working state (the arrays are kept for :meth:`sync_to_host`).
+        ``gforce``: the static gravity force ``(3, nx, ny, nz)`` (ghosted,
+        e.g. :func:`hydropad_b200.ics.static_gravity`), or None."""
         arrs = [np.asfortranarray(a, dtype=np.float64) for a in (p3d, rho3d, vx3d, vy3d, vz3d)]
         nx, ny, nz = arrs[0].shape
         nb = (nx - self.params.shape[0]) // 2
-        L.check(L.lib().hp_attach_state(self._ctx, *[_dptr(a) for a in arrs], None, nx, ny, nz, nb),
-                "hp_attach_state")
+        g = None
+        if gforce is not None:
+            g = np.asfortranarray(gforce, dtype=np.float64)
+            if g.shape != (3, nx, ny, nz):
+                raise ValueError(f"gforce must have shape (3, {nx}, {ny}, {nz})")
+        L.check(L.lib().hp_attach_state(self._ctx, *[_dptr(a) for a in arrs], None if g is None else _dptr(g),
+                                        nx, ny, nz, nb), "hp_attach_state")
         self._host = arrs
+        self._gforce = g
         return arrs
 
     def attach_device(self, p, rho, vx, vy, vz):
@@ -106,6 +115,22 @@ class Hydro:
         L.check(L.lib().hp_attach_device_state(self._ctx, *[C.c_void_p(t.data_ptr()) for t in ts]),
                 "hp_attach_device_state")
         self._host = None
+        self._gforce = None
+
+    def attach_device_gforce(self, gx, gy, gz):
+        """Static gravity force from device tensors (the three components,
+        same layout as :meth:`attach_device`); ``None`` x3 switches it off."""
+        import torch
+        if gx is None:
+            L.check(L.lib().hp_attach_device_gforce(self._ctx, None, None, None), "hp_attach_device_gforce")
+            return
+        shp = tuple(int(v) for v in self.params.shape)[::-1]
+        for t in (gx, gy, gz):
+            if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or tuple(t.shape) != shp:
+                raise ValueError(f"gforce components must be contiguous float64 CUDA tensors of shape {shp}")
+        torch.cuda.current_stream(gx.device).synchronize()
+        L.check(L.lib().hp_attach_device_gforce(self._ctx, *[C.c_void_p(t.data_ptr()) for t in (gx, gy, gz)]),
+                "hp_attach_device_gforce")
 
     def write_var(self, directory: str, fp64: bool = False):
         """The reference's end-of-run dump (write_var_mpi): rho.bin,
@@ -133,7 +158,8 @@ class Hydro:
         nx, ny, nz = (C.c_int(v) for v in a[0].shape)
         nb = C.c_int(self.params.nbound)
         nd = C.c_int(int(ndirection))
-        rc = L.lib().hp_ppmsolver(self._ctx, *[_dptr(x) for x in a], None, None, None,
+        g = getattr(self, "_gforce", None)
+        rc = L.lib().hp_ppmsolver(self._ctx, *[_dptr(x) for x in a], None, None, None if g is None else _dptr(g),
                                   C.byref(nx), C.byref(ny), C.byref(nz), C.byref(nb), C.byref(nd))
         L.check(rc, "hp_ppmsolver")
 

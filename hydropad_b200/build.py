@@ -32,6 +32,9 @@ SOURCES = [
     # differently in different instantiations (tiles, batched or not), and
     # a box must give the same bits whatever tile or batch it runs in.
     ("hp_kernels_mixed.cu", MIXED),
+    # sweeps with the static gravity source, same flags as above
+    ("hp_kernels_grav_fp64.cu", ["--fmad=false"]),
+    ("hp_kernels_grav_mixed.cu", MIXED),
     # persistent batched sweeps (many boxes per launch), same flags as above
     ("hp_batch_fp64.cu", ["--fmad=false"]),
     ("hp_batch_mixed.cu", MIXED),

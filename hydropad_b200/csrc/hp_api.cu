@@ -165,6 +165,54 @@ int enqueue_step(hp_ctx* x, int nrot) {
     return kern + 1;
 }
 
+void drop_gravity(hp_ctx* x) {
+    for (int q = 0; q < 3; ++q) {
+        cudaFree(x->box.g[q]);
+        x->box.g[q] = nullptr;
+    }
+    x->host_g = nullptr;
+}
+
+int alloc_gravity(hp_ctx* x) {
+    const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
+    for (int q = 0; q < 3; ++q)
+        if (!x->box.g[q]) {
+            const int rc = cuda_fail(cudaMalloc(&x->box.g[q], n * sizeof(double)));
+            if (rc != HP_OK) {
+                drop_gravity(x);
+                return rc;
+            }
+        }
+    return HP_OK;
+}
+
+// gforce(3,nx,ny,nz) ghosted Fortran host array -> three dense device
+// components: the interior is copied as 24-byte elements, then split.
+int upload_gforce(hp_ctx* x, const double* gforce, int nxg, int nyg, int nb) {
+    int rc = alloc_gravity(x);
+    if (rc != HP_OK) return rc;
+    const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
+    double* tmp = nullptr;
+    if ((rc = cuda_fail(cudaMalloc(&tmp, 3 * n * sizeof(double)))) != HP_OK) return rc;
+    cudaMemcpy3DParms prm;
+    memset(&prm, 0, sizeof prm);
+    const size_t el = 3 * sizeof(double);
+    prm.srcPtr = make_cudaPitchedPtr((void*)gforce, (size_t)nxg * el, (size_t)nxg, (size_t)nyg);
+    prm.srcPos = make_cudaPos((size_t)nb * el, (size_t)nb, (size_t)nb);
+    prm.dstPtr = make_cudaPitchedPtr((void*)tmp, (size_t)x->box.nx * el, (size_t)x->box.nx, (size_t)x->box.ny);
+    prm.dstPos = make_cudaPos(0, 0, 0);
+    prm.extent = make_cudaExtent((size_t)x->box.nx * el, (size_t)x->box.ny, (size_t)x->box.nz);
+    prm.kind = cudaMemcpyHostToDevice;
+    rc = cuda_fail(cudaMemcpy3DAsync(&prm, x->stream));
+    if (rc == HP_OK && hp::launch_deinterleave3(tmp, x->box.g[0], x->box.g[1], x->box.g[2], (long long)n,
+                                                x->stream) < 0)
+        rc = HP_ERR_CUDA;
+    if (rc == HP_OK) x->launches += 1;
+    cudaStreamSynchronize(x->stream);
+    cudaFree(tmp);
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -284,6 +332,7 @@ int hp_finalize(hp_ctx* x) {
     for (int q = 0; q < 5; ++q) cudaFree(x->box.f[q]);
     for (int q = 0; q < 4; ++q) cudaFree(x->box.snap[q]);
     cudaFree(x->box.peak);
+    for (int q = 0; q < 3; ++q) cudaFree(x->box.g[q]);
     cudaFree(x->box.ctl);
     if (x->ctl_pinned) cudaFreeHost(x->ctl_pinned);
     if (x->stream) cudaStreamDestroy(x->stream);
@@ -320,10 +369,18 @@ int hp_get_scalars(hp_ctx* x, hp_scalars* s) {
 int hp_attach_state(hp_ctx* x, const double* p3d, const double* rho3d, const double* vx3d, const double* vy3d,
                     const double* vz3d, const double* gforce, int nx, int ny, int nz, int nbound) {
     if (!x || !p3d || !rho3d || !vx3d || !vy3d || !vz3d) return HP_ERR_ARG;
-    if (gforce) return HP_ERR_ARG;  // gravity source not supported: configs run without gravity
     if (nbound < 0 || nx != x->box.nx + 2 * nbound || ny != x->box.ny + 2 * nbound || nz != x->box.nz + 2 * nbound)
         return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(x->dev));
+    // gforce is static (initialize_gravity.F90): attaching again with the
+    // same array does not upload it again
+    if (!gforce) {
+        drop_gravity(x);
+    } else if (gforce != x->host_g || !x->box.g[0]) {
+        const int grc = upload_gforce(x, gforce, nx, ny, nbound);
+        if (grc != HP_OK) return grc;
+    }
+    x->host_g = gforce;
     const double* src[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
     for (int q = 0; q < 5; ++q) {
         cudaMemcpy3DParms prm = host_dev_parms(src[q], x->box.f[q], x, nx, ny, nbound, true);
@@ -346,6 +403,8 @@ int hp_attach_device_state(hp_ctx* x, const double* p, const double* rho, const 
     HP_CUDA(cudaSetDevice(x->dev));
     const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
     const double* src[5] = {p, rho, vx, vy, vz};
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    drop_gravity(x);
     for (int q = 0; q < 5; ++q) {
         HP_CUDA(cudaMemcpyAsync(x->box.f[q], src[q], n * sizeof(double), cudaMemcpyDeviceToDevice, x->stream));
         x->host[q] = nullptr;
@@ -374,6 +433,26 @@ int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, doubl
     HP_CUDA(cudaStreamSynchronize(x->stream));
     if (nbound > 0)
         for (int q = 0; q < 5; ++q) fill_ghosts(dst[q], nx, ny, nz, nbound);
+    return HP_OK;
+}
+
+int hp_attach_device_gforce(hp_ctx* x, const double* gx, const double* gy, const double* gz) {
+    if (!x) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    if (!gx && !gy && !gz) {
+        drop_gravity(x);
+        return HP_OK;
+    }
+    if (!gx || !gy || !gz) return HP_ERR_ARG;
+    int rc = alloc_gravity(x);
+    if (rc != HP_OK) return rc;
+    const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
+    const double* src[3] = {gx, gy, gz};
+    for (int q = 0; q < 3; ++q)
+        HP_CUDA(cudaMemcpyAsync(x->box.g[q], src[q], n * sizeof(double), cudaMemcpyDeviceToDevice, x->stream));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    x->host_g = nullptr;
     return HP_OK;
 }
 
@@ -455,8 +534,8 @@ int hp_ppmsolver(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, double* vy
     (void)cho3d;
     (void)nes3d;
     if (!x || !nx || !ny || !nz || !nbound || !ndirection) return HP_ERR_ARG;
-    if (gforce) return HP_ERR_ARG;
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    if (gforce != x->host_g) return HP_ERR_STATE_MISMATCH;  // the attached gforce (or none)
     if (*ndirection < 1 || *ndirection > 3) return HP_ERR_ARG;
     if (*nx != x->hnx || *ny != x->hny || *nz != x->hnz || *nbound != x->hnb) return HP_ERR_STATE_MISMATCH;
     const double* given[5] = {p3d, rho3d, vx3d, vy3d, vz3d};

@@ -15,6 +15,7 @@ struct hp_ctx {
     long long sweep_count;    // selects the rho-bound slot
     long long nstep_host;     // host mirror of the step counter (selects nrot)
     const double* host[5];    // attached host arrays (ghosted, Fortran order)
+    const double* host_g;     // attached host gforce (3,nx,ny,nz), or null
     int hnx, hny, hnz, hnb;
     bool attached;
     int tile[3];              // sweep tile shape per axis (hp_set_tiles / hp_autotune)

@@ -14,7 +14,10 @@
 
 namespace hp {
 
+int launch_sweep_grav_fp64(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st);
+
 int launch_sweep_fp64(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
+    if (b.g[0]) return launch_sweep_grav_fp64(b, axis, tile, bslot, flags, st);
     return launch_sweep_policy<PolicyFP64>(b, axis, tile, bslot, flags, st);
 }
 
@@ -147,6 +150,20 @@ __global__ void timedet_batch_kernel(DevCtl* const* __restrict__ ctls, int n) {
 int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st) {
     if (n <= 0) return 0;
     timedet_batch_kernel<<<(n + 127) / 128, 128, 0, st>>>(ctls, n);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
+__global__ void deinterleave3_kernel(const double* __restrict__ in, double* __restrict__ g0,
+                                     double* __restrict__ g1, double* __restrict__ g2, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        g0[i] = in[3 * i];
+        g1[i] = in[3 * i + 1];
+        g2[i] = in[3 * i + 2];
+    }
+}
+
+int launch_deinterleave3(const double* in, double* g0, double* g1, double* g2, long long n, cudaStream_t st) {
+    deinterleave3_kernel<<<592, 256, 0, st>>>(in, g0, g1, g2, n);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 

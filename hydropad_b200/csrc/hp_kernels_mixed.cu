@@ -14,7 +14,10 @@
 
 namespace hp {
 
+int launch_sweep_grav_mixed(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st);
+
 int launch_sweep_mixed(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
+    if (b.g[0]) return launch_sweep_grav_mixed(b, axis, tile, bslot, flags, st);
     return launch_sweep_policy<PolicyMixed>(b, axis, tile, bslot, flags, st);
 }
 

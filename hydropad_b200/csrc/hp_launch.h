@@ -12,6 +12,7 @@ struct Box {
     double* f[5];      // p, rho, vx, vy, vz (natural order), dense (nx,ny,nz), x fastest
     double* snap[4];   // step-start p, vx, vy, vz (cosmo expand), or null
     double* peak;      // density-peak scratch for y/z sweeps (nx*ny*nz), or null
+    double* g[3];      // gforce components x, y, z (dense, natural layout), or null: gravity off
     DevCtl* ctl;       // device control block
     Consts k;
     int nx, ny, nz;
@@ -39,6 +40,8 @@ int launch_sweep_batch(const BatchLaunch& bl, int axis, int tile, int precision,
 int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st);
 // timedet (advance = 1) on n control blocks.
 int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st);
+// in = (3, n) interleaved (gforce(3,nx,ny,nz) interior) -> g0, g1, g2.
+int launch_deinterleave3(const double* in, double* g0, double* g1, double* g2, long long n, cudaStream_t st);
 // out[i] = (float)in[i], round to nearest even.
 int launch_to_f32(const double* in, float* out, long long n, cudaStream_t st);
 // out[i] = status word of ctls[i], which is cleared.

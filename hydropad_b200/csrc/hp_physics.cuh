@@ -155,20 +155,28 @@ __device__ __forceinline__ double total_energy(double p, double rho, double vx, 
     return p * rgamma1 + 0.5 * rho * (vx * vx + vy * vy + vz * vz);
 }
 
-// integrate, integrate.F90:1-113, without gravity source (g == 0).  f1 is
-// the face at i-1/2, f2 at i+1/2; (u,v,w) are the cell's normal and
-// transverse velocities of this sweep.  pmean, uninitialised in the
-// reference's STENCIL build, is (pm1+pm2)*0.5 as in ppm.F90:583.
+// integrate, integrate.F90:1-113.  f1 is the face at i-1/2, f2 at i+1/2;
+// (u,v,w) are the cell's normal and transverse velocities of this sweep.
+// GRAV adds the source terms of ghalf = -gforce of the cell (:41-44,54-57);
+// without it they are exactly zero and left out.  pmean, uninitialised in
+// the reference's STENCIL build, is (pm1+pm2)*0.5 as in ppm.F90:583.
+template <bool GRAV>
 __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& f2, double& pres, double& rho,
                                           double& u, double& v, double& w, double etot, double eint,
-                                          const Consts& k, const StepScalars& s) {
+                                          const Consts& k, const StepScalars& s, double ghalf) {
     const double gamma = k.gamma, rgamma1 = k.rgamma1, rdtath = s.rdtath, rdx = k.rdx;
     double flux1 = f1.rho * f1.u;
     double flux2 = f2.rho * f2.u;
     double rhonew = rho + rdtath * (flux1 - flux2) * rdx;
     flux1 = f1.rho * f1.u * f1.u + f1.p;
     flux2 = f2.rho * f2.u * f2.u + f2.p;
-    const double vxnew = (u * rho + rdtath * (flux1 - flux2) * rdx) / rhonew;
+    double vxnew;
+    if constexpr (GRAV) {
+        const double grav = (rho + rhonew) * ghalf * 0.5;
+        vxnew = (u * rho + rdtath * (flux1 - flux2) * rdx + rdtath * grav) / rhonew;
+    } else {
+        vxnew = (u * rho + rdtath * (flux1 - flux2) * rdx) / rhonew;
+    }
     flux1 = f1.v * f1.u * f1.rho;
     flux2 = f2.v * f2.u * f2.rho;
     const double vynew = (rho * v + rdtath * (flux1 - flux2) * rdx) / rhonew;
@@ -177,7 +185,13 @@ __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& 
     const double vznew = (rho * w + rdtath * (flux1 - flux2) * rdx) / rhonew;
     flux1 = (gamma * f1.p * rgamma1 + 0.5 * f1.rho * (f1.u * f1.u + f1.v * f1.v + f1.w * f1.w)) * f1.u;
     flux2 = (gamma * f2.p * rgamma1 + 0.5 * f2.rho * (f2.u * f2.u + f2.v * f2.v + f2.w * f2.w)) * f2.u;
-    const double etotnew = etot + rdtath * (flux1 - flux2) * rdx;
+    double etotnew;
+    if constexpr (GRAV) {
+        const double grav = (rho * u + rhonew * vxnew) * ghalf * 0.5;
+        etotnew = etot + rdtath * (flux1 - flux2) * rdx + rdtath * grav;
+    } else {
+        etotnew = etot + rdtath * (flux1 - flux2) * rdx;
+    }
     const double pmean = (f1.p + f2.p) * 0.5;
     double eintnew = eint + rdtath * pmean * (f1.u - f2.u) * rdx;
     flux1 = (f1.p * f1.u) * rgamma1;

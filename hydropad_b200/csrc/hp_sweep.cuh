@@ -46,6 +46,7 @@ struct SweepArgs {
     double* f[5];          // p, rho, u (normal), v, w (transverse) of this sweep
     double* snap[4];       // step-start p, vx, vy, vz (natural order) for expand
     const double* peak;    // per-face density-peak values for y/z sweeps (may be null)
+    const double* g;       // gforce component along this sweep (natural layout), or null: gravity off
     DevCtl* ctl;
     Consts k;
     int nx, ny, nz;
@@ -99,10 +100,13 @@ struct SweepLayout {
     }
 };
 
-template <int AXIS, int P, int T, int RING, class Policy>
+template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
 struct SweepSmem {
     using R = typename Policy::R;
+    static constexpr int kG = GRAV ? P * RING : 1;
     double st[5][P * RING];     // state ring: p, rho, u, v, w
+    double sg[kG];              // gravity ring: g = -gforce of this sweep's axis
+    R slg[kG];                  // ajside slope of g
     R sl[5][P * RING];          // ajside slopes
     R d2[P * RING];             // dda second difference of rho
     unsigned char pf[P * RING]; // flattening flag of pair (c, c+1)
@@ -120,9 +124,9 @@ struct SweepSmem {
 
 // One CTA's worth of work: the P pencils pid0 .. pid0+P-1 of the box `a`,
 // walked from end to end.  Every thread of the CTA calls it.
-template <int AXIS, int P, int T, int RING, class Policy>
+template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
 __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0,
-                                              SweepSmem<AXIS, P, T, RING, Policy>& S) {
+                                              SweepSmem<AXIS, P, T, RING, Policy, GRAV>& S) {
     using R = typename Policy::R;
     using Pow = typename Policy::Pow;
     using CT = typename Policy::CT;
@@ -204,6 +208,12 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             const int ix = L::idx(e, tp);
 #pragma unroll
             for (int q = 0; q < 5; ++q) S.st[q][ix] = v[q];
+            if constexpr (GRAV) {
+                // g(ippm) = -gforce(d, ...) (ppmsolver.F90:108,230,358); the
+                // field never changes, so no save area is needed
+                const int s = e < 0 ? e + N : (e >= N ? e - N : e);
+                S.sg[ix] = -a.g[base + stride * s];
+            }
         }
         __syncthreads();
         // ---------------- A: cell c = e-1 ----------------
@@ -220,6 +230,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                     if (q == 1) S.d2[i0] = dda_second<R>(am, a0, ap, dx_);
                 }
                 S.pf[i0] = flag ? 1 : 0;
+                if constexpr (GRAV) S.slg[i0] = ajside<R>(R(S.sg[im]), R(S.sg[i0]), R(S.sg[ip]));
             }
         }
         __syncthreads();
@@ -289,12 +300,23 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 if (ptr < R(0)) ptr = R(kTiny);
                 if (rtl < R(0)) rtl = R(kTiny);
                 if (rtr < R(0)) rtr = R(kTiny);
-                const R gz = R(0);  // gravity off: g == 0
+                // g at the -/+ characteristics (order2interp.F90:170-172);
+                // gravity off: g == 0
+                R gc1l = R(0), gc3l = R(0), gc1r = R(0), gc3r = R(0);
+                if constexpr (GRAV) {
+                    const Parabola<R> Pg = build_parabola<R>(R(S.sg[ic[1]]), R(S.sg[ic[2]]), R(S.sg[ic[3]]),
+                                                             S.slg[ic[1]], S.slg[ic[2]], S.slg[ic[3]], flat, false,
+                                                             R(0), R(0), dx_);
+                    gc1l = fl(Pg, xm);
+                    gc3l = fl(Pg, xp);
+                    gc1r = fr(Pg, -xm);
+                    gc3r = fr(Pg, -xp);
+                }
                 // left state of face c+1 (order2interp.F90:192-219,249-258)
                 {
                     const R ctl = sqrt(gam_ * ptl * rtl);
-                    const R bm_ = beta<R>(ctl, utl, uc1l, ptl, pc1l, gz, R(-1), dt_, at_, dat_, rat_);
-                    const R bp_ = beta<R>(ctl, utl, uc3l, ptl, pc3l, gz, R(1), dt_, at_, dat_, rat_);
+                    const R bm_ = beta<R>(ctl, utl, uc1l, ptl, pc1l, gc1l, R(-1), dt_, at_, dat_, rat_);
+                    const R bp_ = beta<R>(ctl, utl, uc3l, ptl, pc3l, gc3l, R(1), dt_, at_, dat_, rat_);
                     const R b0_ = beta0<R>(ctl, rtl, rc2l, ptl, pc2l, dt_, at_, dat_);
                     const R bml = (lm > R(0)) ? bm_ : R(0);
                     const R bpl = (lp > R(0)) ? bp_ : R(0);
@@ -316,8 +338,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 // right state of face c (order2interp.F90:221-258)
                 {
                     const R ctr = sqrt(gam_ * ptr * rtr);
-                    const R bp_ = beta<R>(ctr, utr, uc3r, ptr, pc3r, gz, R(1), dt_, at_, dat_, rat_);
-                    const R bm_ = beta<R>(ctr, utr, uc1r, ptr, pc1r, gz, R(-1), dt_, at_, dat_, rat_);
+                    const R bp_ = beta<R>(ctr, utr, uc3r, ptr, pc3r, gc3r, R(1), dt_, at_, dat_, rat_);
+                    const R bm_ = beta<R>(ctr, utr, uc1r, ptr, pc1r, gc1r, R(-1), dt_, at_, dat_, rat_);
                     const R b0_ = beta0<R>(ctr, rtr, rc2r, ptr, pc2r, dt_, at_, dat_);
                     const R bpr = (lp < R(0)) ? bp_ : R(0);
                     const R bmr = (lm < R(0)) ? bm_ : R(0);
@@ -424,7 +446,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                     // the reference gathers these with the x index slot
                     // (ppmsolver.F90:251-252, 379-380); a pre-pass has
                     // evaluated them on the pre-sweep state
-                    const long long wbase = pencil_base<AXIS>((long long)blockIdx.x * P + wtp, a.nx, a.ny);
+                    const long long wbase = pencil_base<AXIS>(pid0 + wtp, a.nx, a.ny);
                     const int fw = f < N ? f : f - N;
                     pk = a.peak[wbase + stride * fw];
                 }
@@ -459,7 +481,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
                 else etot = total_energy(p, rho, u, v, w, k.rgamma1);
                 const double eint = p * k.rgamma1;
-                integrate(f1, f2, p, rho, u, v, w, etot, eint, k, sc);
+                if constexpr (GRAV) integrate<true>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[id]);
+                else integrate<false>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
                 const long long g = base + stride * d;
                 if (a.flags & kFlagExpand) {
                     // expand.F90:161-176 with the step-start snapshot
@@ -509,11 +532,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
 // MINB > 1 asks the compiler for at most 65536/(P*T*MINB) registers per
 // thread so that MINB CTAs fit on one SM (more warps to hide the latency of
 // the FP64 Riemann chains, at the price of spills).
-template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false>
 __global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy>*>(smem_raw);
-    sweep_pencils<AXIS, P, T, RING, Policy>(a, (long long)blockIdx.x * P, S);
+    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy, GRAV>*>(smem_raw);
+    sweep_pencils<AXIS, P, T, RING, Policy, GRAV>(a, (long long)blockIdx.x * P, S);
 }
 
 // Many boxes per launch (the ensemble and the serving batch).  Work item i

@@ -25,6 +25,7 @@ static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int f
     if (axis == 2) { a.f[2] = b.f[4]; a.f[3] = b.f[3]; a.f[4] = b.f[2]; }
     for (int q = 0; q < 4; ++q) a.snap[q] = b.snap[q];
     a.peak = b.peak;
+    a.g = b.g[axis];
     a.ctl = b.ctl;
     a.k = b.k;
     a.nx = b.nx; a.ny = b.ny; a.nz = b.nz;
@@ -35,11 +36,11 @@ static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int f
     return a;
 }
 
-template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1>
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false>
 static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
     const SweepArgs a = make_sweep_args(b, AXIS, bslot, flags);
-    const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy>);
-    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB>;
+    const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy, GRAV>);
+    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB, GRAV>;
     static bool attr_set = false;  // per instantiation (one process drives one device)
     if (!attr_set) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -67,10 +68,11 @@ static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
 HP_TILE_TABLE(HP_TILE_CHECK)
 #undef HP_TILE_CHECK
 
-template <class Policy>
+// GRAV: the instantiation with the gravity source (a box with gforce).
+template <class Policy, bool GRAV = false>
 static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
 #define HP_TILE_CASE(AX, TI, P, T, RING, MINB) \
-    if (axis == AX && tile == TI) return launch_sweep_t<AX, P, T, RING, Policy, MINB>(b, bslot, flags, st);
+    if (axis == AX && tile == TI) return launch_sweep_t<AX, P, T, RING, Policy, MINB, GRAV>(b, bslot, flags, st);
     HP_TILE_TABLE(HP_TILE_CASE)
 #undef HP_TILE_CASE
     return -1;

@@ -152,3 +152,26 @@ def grf_eds_device(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: 
     tcode = temp_k / temperature_factor()
     p = rho * tcode
     return to_dev(p), to_dev(rho), vel[0], vel[1], vel[2]
+
+
+def static_gravity(shape, nb: int = 3, alpha: float = 1.0, sigma: float = float(np.float32(0.3)),
+                   center=(0.5, 0.5, 0.5)):
+    """The reference's static gravity force (initialize_gravity.F90:25-55):
+    a Gaussian potential phi = alpha exp(-r^2 / (2 sigma^2)) about
+    ``center`` at the cell centres x = (i - 0.5) dx (the integer and 0.5
+    in REAL(4), sigma = 0.3 as a REAL(4) literal), and
+    gforce(d) = phi(i+1) - phi(i-1) along d, periodic.  Returns the ghosted
+    ``gforce(3, nx, ny, nz)`` array (component fastest, Fortran order)."""
+    shape = (shape, shape, shape) if np.isscalar(shape) else tuple(int(v) for v in shape)
+    dx = 1.0 / float(max(shape))
+    ax = []
+    for d, n in enumerate(shape):
+        i = np.arange(1, n + 1, dtype=np.float32)
+        ax.append((i - np.float32(0.5)).astype(np.float64) * dx - center[d])
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    phi = alpha * np.exp(-((X * X + Y * Y) + Z * Z) / (2.0 * (sigma * sigma)))
+    g = np.empty((3,) + tuple(n + 2 * nb for n in shape), dtype=np.float64, order="F")
+    for d in range(3):
+        comp = np.roll(phi, -1, axis=d) - np.roll(phi, 1, axis=d)
+        g[d] = np.pad(comp, nb, mode="wrap")
+    return g

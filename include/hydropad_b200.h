@@ -89,8 +89,11 @@ int hp_set_scalars(hp_ctx *ctx, const hp_scalars *s);
 int hp_get_scalars(hp_ctx *ctx, hp_scalars *s);
 
 /* Upload the host state (ghosted Fortran arrays) once; it then stays
- * resident in HBM.  gforce is accepted for ABI compatibility and must be
- * NULL (gravity off). */
+ * resident in HBM.  gforce: the static gravity force gforce(3,nx,ny,nz)
+ * (ghosted, Fortran order, component fastest: hydropad/matrix.F90,
+ * initialize_gravity.F90:49-55), or NULL for no gravity source.  It is
+ * uploaded as three dense components; attaching again with the same gforce
+ * pointer keeps the uploaded copy (the field is static). */
 int hp_attach_state(hp_ctx *ctx, const double *p3d, const double *rho3d,
                     const double *vx3d, const double *vy3d, const double *vz3d,
                     const double *gforce, int nx, int ny, int nz, int nbound);
@@ -104,6 +107,11 @@ int hp_attach_state(hp_ctx *ctx, const double *p3d, const double *rho3d,
  * No counterpart in the reference, whose state is born on the host. */
 int hp_attach_device_state(hp_ctx *ctx, const double *p, const double *rho,
                            const double *vx, const double *vy, const double *vz);
+
+/* The gravity force from DEVICE arrays (three dense components, x fastest,
+ * copied), or all NULL to switch the gravity source off. */
+int hp_attach_device_gforce(hp_ctx *ctx, const double *gx, const double *gy,
+                            const double *gz);
 
 /* Download the resident state into the attached host arrays (interior) and
  * refill their periodic ghost layers. */
@@ -125,8 +133,8 @@ int hp_download_state(hp_ctx *ctx, double *p3d, double *rho3d, double *vx3d,
 
 /* Drop-in for ppmsolver: one directional sweep (1=x, 2=y, 3=z) on the
  * resident state.  The host pointers identify the attached state (they must
- * be the attached arrays); cho3d/nes3d are unused under STENCIL and may be
- * NULL.  Scalars and integers are passed by reference, like the Fortran
+ * be the attached arrays, gforce included, or NULL when none was attached);
+ * cho3d/nes3d are unused under STENCIL and may be NULL.  Scalars and integers are passed by reference, like the Fortran
  * subroutine.  Returns the sweep's error status. */
 int hp_ppmsolver(hp_ctx *ctx, double *p3d, double *rho3d, double *vx3d,
                  double *vy3d, double *vz3d, double *cho3d, double *nes3d,
@@ -194,7 +202,8 @@ int hp_ppmsolver_noalloc(double *p, double *rho, double *vx, double *vy,
  * hp_evolve with the same tiles.
  *
  * Members are contexts created by hp_init on the batch's device with the
- * batch's precision, with their state attached.  Each sweep of a step is
+ * batch's precision, with their state attached and no gravity source
+ * (hp_batch_add returns HP_ERR_ARG otherwise).  Each sweep of a step is
  * one persistent launch per sweep axis over all members, pulling groups of
  * pencils of any member from one work queue.
  * --------------------------------------------------------------------- */

@@ -398,9 +398,10 @@ def integrate(f1, f2, pres, rho, vx, vy, vz, etot, eint, ghalf, S):
     return pnew, rhonew, vxnew, vynew, vznew
 
 
-def ppmsolver(F, nb, nd, S):
+def ppmsolver(F, nb, nd, S, G=None):
     """One STENCIL sweep on ghosted fields F = [p, rho, vx, vy, vz] (numpy,
-    Fortran order); returns updated copies.  Gravity off (g = -0.0)."""
+    Fortran order); returns updated copies.  G: ghosted gforce(3, nx, ny,
+    nz) or None (gravity off: g = -0.0)."""
     p3d, r3d, u3d, v3d, w3d = [a.copy(order="F") for a in F]
     nx, ny, nz = p3d.shape
     A = lambda arr, i, j, k: arr[i - 1, j - 1, k - 1]  # Fortran 1-based
@@ -425,7 +426,7 @@ def ppmsolver(F, nb, nd, S):
                     q = cell(i + ip - 4, a, b)
                     pr_[ip], rh[ip] = A(p3d, *q), A(r3d, *q)
                     vx_[ip], vy_[ip], vz_[ip] = A(roles[0], *q), A(roles[1], *q), A(roles[2], *q)
-                    g_[ip] = np.float64(-0.0)
+                    g_[ip] = np.float64(-0.0) if G is None else -A(G[nd - 1], *q)
                     c_[ip] = np.sqrt(S.gamma * pr_[ip] / rh[ip])
                 faces[(i, a, b)] = order2interp(pr_, rh, vx_, vy_, vz_, g_, c_, S)
     flux = {}
@@ -458,8 +459,9 @@ def ppmsolver(F, nb, nd, S):
                 ux, uy, uz = A(u3d, *q), A(v3d, *q), A(w3d, *q)
                 etot = pz * S.rgamma1 + 0.5 * rz * (ux * ux + uy * uy + uz * uz)
                 eint = pz * S.rgamma1
+                ghalf = -0.0 if G is None else -A(G[nd - 1], *q)
                 res = integrate(flux[(i, a, b)], flux[(i + 1, a, b)], pz, rz, A(roles[0], *q), A(roles[1], *q),
-                                A(roles[2], *q), etot, eint, -0.0, S)
+                                A(roles[2], *q), etot, eint, ghalf, S)
                 idx = tuple(x - 1 for x in q)
                 out_p[idx], out_r[idx] = res[0], res[1]
                 oroles[0][idx], oroles[1][idx], oroles[2][idx] = res[2], res[3], res[4]
@@ -492,27 +494,51 @@ CASES = [
     ("cosmo_x", 4, (10, 8, 6), 1, dict(dt=1.5e-3, at=0.05, dat=3.1, ath=0.0502), dict()),
     ("cosmo_z", 5, (8, 8, 8), 3, dict(dt=1.5e-3, at=0.05, dat=3.1, ath=0.0502), dict()),
     ("peak_y", 6, (10, 10, 10), 2, dict(dt=1e-3, at=1.0, dat=0.0, ath=1.0), dict(dmax=2.0)),
+    # static gravity source (the Gaussian potential of initialize_gravity.F90,
+    # scaled up so the source terms are large)
+    ("grav_x", 7, (10, 8, 6), 1, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
+    ("grav_y", 8, (8, 10, 6), 2, dict(dt=1.5e-3, at=0.05, dat=3.1, ath=0.0502), dict()),
+    ("grav_z", 9, (6, 8, 10), 3, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
 ]
+
+
+def gravity_field(shape, nb, alpha=40.0, sigma=0.3):
+    """gforce(3, ...) ghosted: phi = alpha exp(-r^2/(2 sigma^2)) at the cell
+    centres, central differences phi(i+1) - phi(i-1), periodic."""
+    dx = 1.0 / max(shape)
+    ax = [(np.arange(n) + 0.5) * dx - 0.5 for n in shape]
+    X, Y, Z = np.meshgrid(*ax, indexing="ij")
+    phi = alpha * np.exp(-(X * X + Y * Y + Z * Z) / (2.0 * sigma * sigma))
+    g = np.empty((3,) + tuple(n + 2 * nb for n in shape), order="F")
+    for d in range(3):
+        g[d] = np.pad(np.roll(phi, -1, axis=d) - np.roll(phi, 1, axis=d), nb, mode="wrap")
+    return g
 
 
 def run_case(name, seed, shape, nd, tsc, extra):
     nb = 3
     F = make_case(seed, shape, nb, peak=name.startswith("peak"))
     S = Sc(5.0 / 3.0, 1.0 / max(shape), **tsc, **extra)
-    out = ppmsolver(F, nb, nd, S)
-    return F, out, S
+    G = gravity_field(shape, nb) if name.startswith("grav") else None
+    out = ppmsolver(F, nb, nd, S, G)
+    return F, out, S, G
 
 
-def main():
+def main(names=None):
+    """Write the golden files of the named cases (default: all)."""
     np.seterr(all="ignore")  # IEEE results (inf/NaN) instead of warnings, as in Fortran
     here = os.path.dirname(os.path.abspath(__file__))
     for name, seed, shape, nd, tsc, extra in CASES:
-        F, out, S = run_case(name, seed, shape, nd, tsc, extra)
+        if names and name not in names:
+            continue
+        F, out, S, G = run_case(name, seed, shape, nd, tsc, extra)
+        more = {} if G is None else {"gforce": G}
         np.savez_compressed(os.path.join(here, f"{name}.npz"), inp=np.stack(F), out=np.stack(out), nd=nd,
                             shape=np.array(shape), dt=tsc["dt"], at=tsc["at"], dat=tsc["dat"], ath=tsc["ath"],
-                            dmax=extra.get("dmax", 2e10))
+                            dmax=extra.get("dmax", 2e10), **more)
         print(name, "ok")
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+    main(sys.argv[1:])

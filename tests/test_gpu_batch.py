@@ -138,3 +138,39 @@ def test_batch_rejects_mismatch():
         b.remove(h1)
         for h in (h64, h1, h2):
             h.close()
+
+
+def test_batch_density_peak_fix_matches_alone():
+    """With dmax low enough for the density-peak fix (riemannsolver.F90:
+    279-285) to act, batched y/z sweeps read the pre-pass values of their
+    own pencils: bitwise equal to the boxes alone."""
+    from hydropad_b200.api import Hydro
+    from hydropad_b200.batch import Batch
+    specs = [(24, 31), (16, 32), (20, 33)]
+    steps = 4
+
+    def make(n, seed, dmax):
+        h = Hydro(params_for((n, n, n), cosmo=True, dmax=dmax), precision="fp64")
+        h.attach_state(*grf_state(n, seed=seed))
+        h.set_tiles(*TILES)
+        h.start_with_cfl()
+        return h
+
+    alone, plain = [], []
+    for n, seed in specs:
+        for dmax, out in ((1.5, alone), (2e10, plain)):
+            with make(n, seed, dmax) as h:
+                h.evolve(steps)
+                out.append(h.download())
+    assert any(not np.array_equal(a[0], b[0]) for a, b in zip(alone, plain)), "the fix never acted"
+    boxes = [make(n, seed, 1.5) for n, seed in specs]
+    with Batch("fp64", capacity=4) as b:
+        b.set_tiles(*TILES)
+        for h in boxes:
+            b.add(h)
+        b.step(steps)
+        b.synchronize()
+        for h, ref in zip(boxes, alone):
+            _same(h.download(), ref, "peak")
+            b.remove(h)
+            h.close()

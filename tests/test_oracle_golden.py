@@ -38,7 +38,7 @@ def oracle_scalars(oracle, z):
 @pytest.mark.parametrize("name", golden_cases())
 def test_oracle_matches_golden(oracle, name):
     z, inp, out = load_case(name)
-    st = oracle.OracleState(*inp)
+    st = oracle.OracleState(*inp, gforce=z["gforce"] if "gforce" in z.files else None)
     s = oracle_scalars(oracle, z)
     assert st.ppmsolver(s, int(z["nd"])) == 0
     for q in range(5):
@@ -47,7 +47,13 @@ def test_oracle_matches_golden(oracle, name):
 
 
 def test_golden_set_present():
-    assert len(GOLDEN) >= 6, "run tests/golden/gen_golden.py"
+    assert len(GOLDEN) >= 9, "run tests/golden/gen_golden.py"
+
+
+def test_gravity_cases_have_a_source():
+    for name in ("grav_x", "grav_y", "grav_z"):
+        z, _, _ = load_case(name)
+        assert np.abs(z["gforce"]).max() > 0.1
 
 
 def test_peak_case_exercises_the_fix():
