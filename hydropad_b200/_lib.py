@@ -51,7 +51,7 @@ EXPORTS = (
     "hp_download_state", "hp_ppmsolver", "hp_ppm_lxlylz", "hp_speed", "hp_timedet", "hp_evolve",
     "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count", "hp_set_tiles",
     "hp_get_tiles", "hp_autotune", "hp_ppmsolver_noalloc", "hp_attach_device_state",
-    "hp_write_var", "hp_evolve_async", "hp_attach_device_gforce",
+    "hp_write_var", "hp_evolve_async", "hp_attach_device_gforce", "hp_num_tiles",
     "hp_batch_create", "hp_batch_destroy", "hp_batch_add", "hp_batch_remove", "hp_batch_size",
     "hp_batch_step", "hp_batch_synchronize", "hp_batch_member", "hp_batch_set_tiles", "hp_batch_get_tiles",
     "hp_batch_autotune", "hp_batch_stream", "hp_batch_launch_count",
@@ -80,6 +80,7 @@ def lib():
     L.hp_attach_state.argtypes = [cp, dp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.hp_attach_device_state.argtypes = [cp, cp, cp, cp, cp, cp]
     L.hp_write_var.argtypes = [cp, C.c_char_p, C.c_int]
+    L.hp_num_tiles.argtypes = []
     L.hp_attach_device_gforce.argtypes = [cp, cp, cp, cp]
     L.hp_sync_to_host.argtypes = [cp]
     L.hp_download_state.argtypes = [cp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int]
@@ -123,6 +124,11 @@ def lib():
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
+
+
+def num_tiles() -> int:
+    """Tile shapes per axis of the sweep kernels."""
+    return int(lib().hp_num_tiles())
 
 
 def check(rc: int, what: str = "") -> None:

@@ -657,6 +657,8 @@ int hp_set_tiles(hp_ctx* x, int tile_x, int tile_y, int tile_z) {
     return HP_OK;
 }
 
+int hp_num_tiles(void) { return hp::kNumTiles; }
+
 int hp_get_tiles(hp_ctx* x, int* tiles) {
     if (!x || !tiles) return HP_ERR_ARG;
     for (int a = 0; a < 3; ++a) tiles[a] = x->tile[a];

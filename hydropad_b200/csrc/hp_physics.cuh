@@ -160,7 +160,12 @@ __device__ __forceinline__ double total_energy(double p, double rho, double vx, 
 // GRAV adds the source terms of ghalf = -gforce of the cell (:41-44,54-57);
 // without it they are exactly zero and left out.  pmean, uninitialised in
 // the reference's STENCIL build, is (pm1+pm2)*0.5 as in ppm.F90:583.
-template <bool GRAV>
+// Div::div(a, b) is the division: IEEE for the FP64 path, a refined
+// hardware reciprocal for the mixed path.
+struct DivIEEE {
+    __device__ __forceinline__ static double div(double a, double b) { return a / b; }
+};
+template <bool GRAV, class Div = DivIEEE>
 __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& f2, double& pres, double& rho,
                                           double& u, double& v, double& w, double etot, double eint,
                                           const Consts& k, const StepScalars& s, double ghalf) {
@@ -173,16 +178,16 @@ __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& 
     double vxnew;
     if constexpr (GRAV) {
         const double grav = (rho + rhonew) * ghalf * 0.5;
-        vxnew = (u * rho + rdtath * (flux1 - flux2) * rdx + rdtath * grav) / rhonew;
+        vxnew = Div::div(u * rho + rdtath * (flux1 - flux2) * rdx + rdtath * grav, rhonew);
     } else {
-        vxnew = (u * rho + rdtath * (flux1 - flux2) * rdx) / rhonew;
+        vxnew = Div::div(u * rho + rdtath * (flux1 - flux2) * rdx, rhonew);
     }
     flux1 = f1.v * f1.u * f1.rho;
     flux2 = f2.v * f2.u * f2.rho;
-    const double vynew = (rho * v + rdtath * (flux1 - flux2) * rdx) / rhonew;
+    const double vynew = Div::div(rho * v + rdtath * (flux1 - flux2) * rdx, rhonew);
     flux1 = f1.w * f1.u * f1.rho;
     flux2 = f2.w * f2.u * f2.rho;
-    const double vznew = (rho * w + rdtath * (flux1 - flux2) * rdx) / rhonew;
+    const double vznew = Div::div(rho * w + rdtath * (flux1 - flux2) * rdx, rhonew);
     flux1 = (gamma * f1.p * rgamma1 + 0.5 * f1.rho * (f1.u * f1.u + f1.v * f1.v + f1.w * f1.w)) * f1.u;
     flux2 = (gamma * f2.p * rgamma1 + 0.5 * f2.rho * (f2.u * f2.u + f2.v * f2.v + f2.w * f2.w)) * f2.u;
     double etotnew;
@@ -201,9 +206,9 @@ __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& 
     // dual energy, :85-98 (STENCIL: ee2 = etotnew)
     const double vvv = vxnew * vxnew + vynew * vynew + vznew * vznew;
     const double eeaux = etotnew - 0.5 * rhonew * vvv;
-    const double ee1 = eeaux / etotnew;
+    const double ee1 = Div::div(eeaux, etotnew);
     if (ee1 >= k.eta2) eintnew = eeaux;
-    const double ee0 = eeaux / etotnew;
+    const double ee0 = Div::div(eeaux, etotnew);
     double pnew;
     if (ee0 >= k.eta1) pnew = (gamma - 1.0) * eeaux;
     else pnew = (gamma - 1.0) * eintnew;

@@ -65,6 +65,7 @@ struct PolicyFP64 {
     using PowC = PowRoot;
     using RareT = double;      // closed two-rarefaction form
     using PowRare = PowRoot;
+    using DivD = DivIEEE;      // divisions of the update
 };
 // Mixed precision: reconstruction, flattening, characteristic tracing and
 // the traced face states in FP32; the Riemann solver's Newton for p*, u*,
@@ -77,6 +78,7 @@ struct PolicyMixed {
     using PowC = PowF32m;
     using RareT = float;         // closed two-rarefaction form: no iteration
     using PowRare = PowRareF32;
+    using DivD = PowRootShort;   // update divisions from a refined reciprocal (an ulp or two)
 };
 
 template <int AXIS>
@@ -392,27 +394,28 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 if (mycase == c4) rank = __popc(m & lt);
             }
             __syncthreads();
-            if (mycase) {
-                int off = 0;
+            {
+                // offset of (pattern, warp) in the sorted list: every warp
+                // scans the per-warp counts itself (lane w holds warp w's
+                // count), pattern after pattern
+                constexpr int kW = L::kThreads / 32;
+                static_assert(kW <= 32, "one lane per warp");
+                int base_off = 0, my_off = 0;
+#pragma unroll
                 for (int c4 = 0; c4 < 5; ++c4) {
-                    int tot = 0, before = 0;
-                    for (int w = 0; w < L::kThreads / 32; ++w) {
-                        tot += S.cnt[w][c4];
-                        before += (w < warp) ? S.cnt[w][c4] : 0;
+                    const int v = lane < kW ? S.cnt[lane][c4] : 0;
+                    int incl = v;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                        if (lane >= o) incl += u;
                     }
-                    if (c4 + 1 == mycase) {
-                        off += before;
-                        break;
-                    }
-                    off += tot;
+                    const int excl_w = __shfl_sync(0xffffffffu, incl - v, warp);  // warps before mine
+                    if (c4 + 1 == mycase) my_off = base_off + excl_w;
+                    base_off += __shfl_sync(0xffffffffu, incl, 31);           // all warps
                 }
-                S.work[off + rank] = (mycase << 24) | (tp << 16) | f;  // (pattern, pencil, face)
-            }
-            if (tid == 0) {
-                int tot = 0;
-                for (int w = 0; w < L::kThreads / 32; ++w)
-                    for (int c4 = 0; c4 < 5; ++c4) tot += S.cnt[w][c4];
-                S.nwork = tot;
+                if (mycase) S.work[my_off + rank] = (mycase << 24) | (tp << 16) | f;  // (pattern, pencil, face)
+                if (tid == 0) S.nwork = base_off;
             }
         }
         __syncthreads();
@@ -481,8 +484,9 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
                 else etot = total_energy(p, rho, u, v, w, k.rgamma1);
                 const double eint = p * k.rgamma1;
-                if constexpr (GRAV) integrate<true>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[id]);
-                else integrate<false>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
+                using DivD = typename Policy::DivD;
+                if constexpr (GRAV) integrate<true, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[id]);
+                else integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
                 const long long g = base + stride * d;
                 if (a.flags & kFlagExpand) {
                     // expand.F90:161-176 with the step-start snapshot

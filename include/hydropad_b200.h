@@ -162,7 +162,11 @@ int hp_evolve(hp_ctx *ctx, int nsteps, int use_graph);
  * are enqueued on the context's stream (hp_synchronize reads the status). */
 int hp_evolve_async(hp_ctx *ctx, int nsteps, int use_graph);
 
-/* Sweep tile shape per axis (0 .. 7; pencils per CTA x cells per window
+/* Number of sweep tile shapes per axis (the valid tile indices are
+ * 0 .. hp_num_tiles()-1). */
+int hp_num_tiles(void);
+
+/* Sweep tile shape per axis (0 .. hp_num_tiles()-1; pencils per CTA x cells per window
  * step).  Results do not depend on the tile, only the speed does.  No
  * reference counterpart (the reference leaves the launch shape to PGI's
  * OpenACC compiler, ppmsolver.F90:96 `!num_gangs ... vector_length`). */
@@ -236,7 +240,7 @@ int hp_batch_step(hp_batch *b, int nsteps, int use_graph);
 int hp_batch_synchronize(hp_batch *b, int *status);
 hp_ctx *hp_batch_member(hp_batch *b, int i);
 
-/* Tile shape per axis of the batched sweeps (0 .. 7, as hp_set_tiles), and
+/* Tile shape per axis of the batched sweeps (as hp_set_tiles), and
  * the autotuner over the current members (on scratch copies of their
  * states; the states are not changed). */
 int hp_batch_set_tiles(hp_batch *b, int tile_x, int tile_y, int tile_z);
