@@ -45,13 +45,13 @@ __device__ __forceinline__ double ipow_fixed(double y) {
     for (int i = 1; i < N; ++i) r *= y;
     return r;
 }
-template <int N>
+template <int N, int STEPS = 2>
 __device__ __forceinline__ double inv_root_fixed(double x) {
     if (!(x > 1e-30 && x < 1e30)) return pow_shared(x, -1.0 / (double)N);
     double z = (double)exp2f(__log2f((float)x) * (-1.0f / (float)N));
     constexpr double rn = 1.0 / (double)N;
 #pragma unroll
-    for (int it = 0; it < 2; ++it) z = z + z * ((1.0 - x * ipow_fixed<N>(z)) * rn);
+    for (int it = 0; it < STEPS; ++it) z = z + z * ((1.0 - x * ipow_fixed<N>(z)) * rn);
     return z;
 }
 static __device__ __noinline__ double inv_root_any(double x, int n) {
@@ -62,8 +62,9 @@ static __device__ __noinline__ double inv_root_any(double x, int n) {
     return z;
 }
 // x^(-(n-1)/n) = x^-gf, the common factor of every power below
+template <int STEPS = 2>
 __device__ __forceinline__ double pow_mgf(double x, int n) {
-    if (n == 5) return ipow_fixed<4>(inv_root_fixed<5>(x));
+    if (n == 5) return ipow_fixed<4>(inv_root_fixed<5, STEPS>(x));
     return ipow(inv_root_any(x, n), n - 1);
 }
 
@@ -73,18 +74,18 @@ __device__ __forceinline__ double pow_mgf(double x, int n) {
 // every power follows from z = x^(-1/n):  x^-gf = z^(n-1),
 // x^m = x z^(n-1), x^rgamma = (x^m)^j, x^rm = x^n.  These agree with pow()
 // to a few ulp.  Other gammas use pow().
-struct PowRoot {
-    static constexpr bool kShortNewton = false;  // literal riemann.F90 loop body
+template <int STEPS>  // Newton steps of the fifth root
+struct PowRootBase {
     __device__ __forceinline__ static double pm(double x, const Consts& k) {
-        return k.nroot ? x * pow_mgf(x, k.nroot) : pow_shared(x, k.m);
+        return k.nroot ? x * pow_mgf<STEPS>(x, k.nroot) : pow_shared(x, k.m);
     }
     __device__ __forceinline__ static double pgf(double x, const Consts& k) {
-        return k.nroot ? pow_mgf(x, k.nroot) : pow_shared(x, -k.gf);
+        return k.nroot ? pow_mgf<STEPS>(x, k.nroot) : pow_shared(x, -k.gf);
     }
     // x^m and x^-gf from one root
     __device__ __forceinline__ static void pm_pgf(double x, double& m_, double& gf_, const Consts& k) {
         if (k.nroot) {
-            gf_ = pow_mgf(x, k.nroot);
+            gf_ = pow_mgf<STEPS>(x, k.nroot);
             m_ = x * gf_;
         } else {
             m_ = pow_shared(x, k.m);
@@ -99,7 +100,11 @@ struct PowRoot {
         if (k.nroot == 5) return ipow_fixed<5>(x);
         return k.nroot ? ipow(x, k.nroot) : pow_shared(x, k.rm);
     }
-    // IEEE division
+};
+
+// FP64 path: roots to a few ulp, IEEE division, the literal loop body.
+struct PowRoot : PowRootBase<2> {
+    static constexpr bool kShortNewton = false;  // literal riemann.F90 loop body
     __device__ __forceinline__ static double div(double a, double b) { return a / b; }
 };
 
@@ -114,12 +119,22 @@ __device__ __forceinline__ double rcp_refined(double b) {
     e = fma(-b, r, 1.0);
     return fma(r, e, r);
 }
-struct PowRootShort : PowRoot {
+// The powers of the mixed path take one Newton step from the FP32 root
+// estimate (relative error ~1e-13, far inside the 1e-3 step tolerance of
+// the Newton iteration that uses them), and the divisions inside the loop
+// one step from the hardware reciprocal (div_loop, ~1e-13).
+struct PowRootShort : PowRootBase<1> {
     static constexpr bool kShortNewton = true;
     __device__ __forceinline__ static double div(double a, double b) {
         const double r = rcp_refined(b);
         const double q = a * r;
         return fma(r, fma(-b, q, a), q);
+    }
+    __device__ __forceinline__ static double div_loop(double a, double b) {
+        double r;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+        r = fma(r, fma(-b, r, 1.0), r);
+        return a * r;
     }
 };
 
@@ -189,60 +204,49 @@ __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vsta
     const double cright = sqrt(k.gamma * pright * rhoright);
     const double rpl = Pow::div(1.0, pleft), rpr = Pow::div(1.0, pright);
     const double rcl = Pow::div(1.0, cleft), rcr = Pow::div(1.0, cright);
-    double a = 0.0, b = 0.0;
+    // only 1/a and 1/b enter the iteration; u* = (pL-pR + a uL + b uR)/(a+b)
+    // is formed once at the end from them
+    double ia = 0.0, ib = 0.0;
+    bool ok = false;
     for (int nnewt = 1; nnewt <= kNewtonMax; ++nnewt) {
         const double pstarold = pstar;
         const double rl = pstar * rpl, rr = pstar * rpr;
-        double ia, ib, vprimel, vprimer;
+        double vprimel, vprimer;
         if (pstar >= pleft) {
             const double q = k.gf * rl + k.m, rs = rsqrt(q);
-            a = cleft * q * rs;
             ia = rs * rcl;
             const double ca = cleft * ia;
             vprimel = -0.5 * ia * (1.0 + ca * ca);
         } else {
             double pw, pg;
             Pow::pm_pgf(rl, pw, pg, k);
-            if ((1.0 - pw) == 0.0) {
-                const double q = k.gf * rl + k.m, rs = rsqrt(q);
-                a = cleft * q * rs;
-                ia = rs * rcl;
-            } else {
-                ia = Pow::div(1.0 - pw, k.m * cleft * (1.0 - rl));
-                a = Pow::div(k.m * cleft * (1.0 - rl), 1.0 - pw);
-            }
+            if ((1.0 - pw) == 0.0) ia = rsqrt(k.gf * rl + k.m) * rcl;
+            else ia = Pow::div_loop(1.0 - pw, k.m * cleft * (1.0 - rl));
             vprimel = -(rcl * pg);  // (1/cl) rl^-gf
         }
         if (pstar >= pright) {
             const double q = k.gf * rr + k.m, rs = rsqrt(q);
-            b = cright * q * rs;
             ib = rs * rcr;
             const double cb = cright * ib;
             vprimer = 0.5 * ib * (1.0 + cb * cb);
         } else {
             double pw, pg;
             Pow::pm_pgf(rr, pw, pg, k);
-            if ((1.0 - pw) == 0.0) {
-                const double q = k.gf * rr + k.m, rs = rsqrt(q);
-                b = cright * q * rs;
-                ib = rs * rcr;
-            } else {
-                ib = Pow::div(1.0 - pw, k.m * cright * (1.0 - rr));
-                b = Pow::div(k.m * cright * (1.0 - rr), 1.0 - pw);
-            }
+            if ((1.0 - pw) == 0.0) ib = rsqrt(k.gf * rr + k.m) * rcr;
+            else ib = Pow::div_loop(1.0 - pw, k.m * cright * (1.0 - rr));
             vprimer = rcr * pg;
         }
         const double vstarl = vxleft - (pstar - pleft) * ia;
         const double vstarr = vxright + (pstar - pright) * ib;
-        pstar = pstar - Pow::div(vstarl - vstarr, vprimel - vprimer);
+        pstar = pstar - Pow::div_loop(vstarl - vstarr, vprimel - vprimer);
         if (pstar <= 0.0) pstar = pstarold * 0.001;
         if (!(fabs(pstarold - pstar) > kTerr * pstarold)) {
-            vstar = Pow::div(pleft - pright + a * vxleft + b * vxright, a + b);
-            return true;
+            ok = true;
+            break;
         }
     }
-    vstar = Pow::div(pleft - pright + a * vxleft + b * vxright, a + b);
-    return false;
+    vstar = Pow::div((pleft - pright) * ia * ib + vxleft * ib + vxright * ia, ia + ib);
+    return ok;
 }
 
 template <class Pow>
@@ -324,9 +328,19 @@ __device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, co
                                                           const Consts& k) {
     const double gamma = k.gamma;
     const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
-    pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
-                      (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
-                  k);
+    // the start value riemann.F90 replaces by its guess when that is
+    // positive; the mixed path's guess is positive for almost every face,
+    // so it forms this one only when it is needed
+    bool need_start = true;
+    if constexpr (Pow::kShortNewton) {
+        const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
+        need_start = !(0.5 * (pleft + pright) + 0.5 * kappa * (vxleft - vxright) > 0.0);
+        pm = 0.0;
+    }
+    if (need_start)
+        pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
+                          (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
+                      k);
     const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
     if (pleft >= pright) {
         const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
