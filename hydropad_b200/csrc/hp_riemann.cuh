@@ -13,11 +13,13 @@
 
 namespace hp {
 
-__device__ __forceinline__ double rarwave(double f1, double f2, double vt, double vh) {  // :290-298
+template <class S = double>
+__device__ __forceinline__ S rarwave(S f1, S f2, S vt, S vh) {  // :290-298
     return f2 + vt * (f1 - f2) / (vt - vh);
 }
-__device__ __forceinline__ double rhoshock(double p2, double p1, double rho1, double gamma1) {  // :303-313
-    return rho1 * (gamma1 * p2 / p1 + 1.0) / (gamma1 + p2 / p1);
+template <class S = double>
+__device__ __forceinline__ S rhoshock(S p2, S p1, S rho1, S gamma1) {  // :303-313
+    return rho1 * (gamma1 * p2 / p1 + S(1)) / (gamma1 + p2 / p1);
 }
 
 // ------------------------------------------------------------------------
@@ -300,29 +302,35 @@ __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, dou
     return true;
 }
 
-// Pattern 1: two shocks, riemannsolver.F90:73-109.
-template <class Pow>
+// Pattern 1: two shocks, riemannsolver.F90:73-109.  The Newton iteration
+// for p*, u* runs in FP64; S is the type of the sampling that follows it
+// (which wave lands on the face, and the density behind it): double in the
+// FP64 path, float in the mixed path, as its closed two-rarefaction form.
+template <class Pow, class S = double>
 __device__ __forceinline__ bool riemann_two_shocks(const FaceState& L, const FaceState& R, double& pm, double& vxm,
                                                    double& rhom, const Consts& k) {
     const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
     pm = fmax2(pleft, pright);
     const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
-    const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
-    const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
-    double vshock1, vshock2;
-    if (rhoshock1 == rholeft) vshock1 = 0.0;
-    else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
-    if (rhoshock2 == rhoright) vshock2 = 0.0;
-    else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
-    if (vshock2 < 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-    else if (vxm <= 0.0 && vshock2 >= 0.0) rhom = rhoshock2;
-    else if (vshock1 <= 0.0 && vxm > 0.0) rhom = rhoshock1;
+    const S pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
+    const S rl = S(rholeft), rr = S(rhoright);
+    const S rhoshock1 = rhoshock<S>(pmS, S(pleft), rl, g1);
+    const S rhoshock2 = rhoshock<S>(pmS, S(pright), rr, g1);
+    S vshock1, vshock2;
+    if (rhoshock1 == rl) vshock1 = S(0);
+    else vshock1 = (rhoshock1 * vxmS - rl * S(vxleft)) / (rhoshock1 - rl);
+    if (rhoshock2 == rr) vshock2 = S(0);
+    else vshock2 = (rhoshock2 * vxmS - rr * S(vxright)) / (rhoshock2 - rr);
+    if (vshock2 < S(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
+    else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = double(rhoshock2);
+    else if (vshock1 <= S(0) && vxm > 0.0) rhom = double(rhoshock1);
     else { pm = pleft; vxm = vxleft; rhom = rholeft; }
     return ok;
 }
 
 // Pattern 2: one shock and one rarefaction, riemannsolver.F90:113-184.
-template <class Pow>
+// Newton in FP64, sampling in S with the powers of PowS (as pattern 1).
+template <class Pow, class S = double, class PowS = Pow>
 __device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, const FaceState& R, double cleft,
                                                           double cright, double& pm, double& vxm, double& rhom,
                                                           const Consts& k) {
@@ -342,39 +350,42 @@ __device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, co
                           (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
                       k);
     const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+    const S gS = S(gamma), pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
     if (pleft >= pright) {
-        const double rhoshock2 = rhoshock(pm, pright, rhoright, k.gamma1);
-        const double rhocont1 = rholeft * Pow::prg(pm / pleft, k);
-        double vshock2;
-        if (rhoshock2 == rhoright) vshock2 = 0.0;
-        else vshock2 = (rhoshock2 * vxm - rhoright * vxright) / (rhoshock2 - rhoright);
-        const double vtail1 = vxm - sqrt(gamma * pm / rhocont1);
-        const double vhead1 = vxleft - cleft;
-        if (vshock2 < 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-        else if (vhead1 >= 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-        else if (vxm <= 0.0 && vshock2 >= 0.0) rhom = rhoshock2;
-        else if (vxm > 0.0 && vtail1 <= 0.0) rhom = rhocont1;
-        else if (vtail1 > 0.0 && vhead1 <= 0.0) {
-            pm = rarwave(pleft, pm, vtail1, vhead1);
-            rhom = rarwave(rholeft, rhocont1, vtail1, vhead1);
-            vxm = rarwave(vxleft, vxm, vtail1, vhead1);
+        const S rr = S(rhoright), rl = S(rholeft);
+        const S rhoshock2 = rhoshock<S>(pmS, S(pright), rr, g1);
+        const S rhocont1 = rl * PowS::prg(pmS / S(pleft), k);
+        S vshock2;
+        if (rhoshock2 == rr) vshock2 = S(0);
+        else vshock2 = (rhoshock2 * vxmS - rr * S(vxright)) / (rhoshock2 - rr);
+        const S vtail1 = vxmS - sqrt(gS * pmS / rhocont1);
+        const S vhead1 = S(vxleft) - S(cleft);
+        if (vshock2 < S(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
+        else if (vhead1 >= S(0)) { pm = pleft; vxm = vxleft; rhom = rholeft; }
+        else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = double(rhoshock2);
+        else if (vxm > 0.0 && vtail1 <= S(0)) rhom = double(rhocont1);
+        else if (vtail1 > S(0) && vhead1 <= S(0)) {
+            pm = double(rarwave<S>(S(pleft), pmS, vtail1, vhead1));
+            rhom = double(rarwave<S>(rl, rhocont1, vtail1, vhead1));
+            vxm = double(rarwave<S>(S(vxleft), vxmS, vtail1, vhead1));
         }
     } else {
-        const double rhoshock1 = rhoshock(pm, pleft, rholeft, k.gamma1);
-        const double rhocont2 = rhoright * Pow::prg(pm / pright, k);
-        double vshock1;
-        if (rhoshock1 == rholeft) vshock1 = 0.0;
-        else vshock1 = (rhoshock1 * vxm - rholeft * vxleft) / (rhoshock1 - rholeft);
-        const double vtail2 = vxm + sqrt(gamma * pm / rhocont2);
-        const double vhead2 = vxright + cright;
-        if (vshock1 > 0.0) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-        else if (vhead2 <= 0.0) { pm = pright; vxm = vxright; rhom = rhoright; }
-        else if (vxm >= 0.0 && vshock1 <= 0.0) rhom = rhoshock1;
-        else if (vxm < 0.0 && vtail2 >= 0.0) rhom = rhocont2;
-        else if (vtail2 < 0.0 && vhead2 >= 0.0) {
-            pm = rarwave(pright, pm, vtail2, vhead2);
-            rhom = rarwave(rhoright, rhocont2, vtail2, vhead2);
-            vxm = rarwave(vxright, vxm, vtail2, vhead2);
+        const S rr = S(rhoright), rl = S(rholeft);
+        const S rhoshock1 = rhoshock<S>(pmS, S(pleft), rl, g1);
+        const S rhocont2 = rr * PowS::prg(pmS / S(pright), k);
+        S vshock1;
+        if (rhoshock1 == rl) vshock1 = S(0);
+        else vshock1 = (rhoshock1 * vxmS - rl * S(vxleft)) / (rhoshock1 - rl);
+        const S vtail2 = vxmS + sqrt(gS * pmS / rhocont2);
+        const S vhead2 = S(vxright) + S(cright);
+        if (vshock1 > S(0)) { pm = pleft; vxm = vxleft; rhom = rholeft; }
+        else if (vhead2 <= S(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
+        else if (vxm >= 0.0 && vshock1 <= S(0)) rhom = double(rhoshock1);
+        else if (vxm < 0.0 && vtail2 >= S(0)) rhom = double(rhocont2);
+        else if (vtail2 < S(0) && vhead2 >= S(0)) {
+            pm = double(rarwave<S>(S(pright), pmS, vtail2, vhead2));
+            rhom = double(rarwave<S>(rr, rhocont2, vtail2, vhead2));
+            vxm = double(rarwave<S>(S(vxright), vxmS, vtail2, vhead2));
         }
     }
     return ok;
@@ -476,7 +487,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
     double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
     bool ok = true;
     if (pattern == 1) {
-        ok = riemann_two_shocks<Pow>(L, R, pm, vxm, rhom, k);
+        ok = riemann_two_shocks<Pow, RareT>(L, R, pm, vxm, rhom, k);
     } else if (pattern == 3) {
         const RareT g = RareT(k.gamma);
         const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);
@@ -504,7 +515,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
         }
     } else if (pattern == 2 || pattern == 4) {
         const double cleft = sqrt(k.gamma * L.p / L.rho), cright = sqrt(k.gamma * R.p / R.rho);
-        if (pattern == 2) ok = riemann_shock_rarefaction<Pow>(L, R, cleft, cright, pm, vxm, rhom, k);
+        if (pattern == 2) ok = riemann_shock_rarefaction<Pow, RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
         else riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
     }
     riemann_finish(L, R, pm, vxm, rhom, out, s);
