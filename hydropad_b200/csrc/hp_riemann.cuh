@@ -182,26 +182,50 @@ struct PowF32m {
 // riemann, riemann.F90:318-400 (van Leer Newton for p*).  Returns false when
 // more than 100 iterations would be needed (the reference stops the run).
 // ------------------------------------------------------------------------
+// Start value of the mixed path's Newton iteration: the two-rarefaction
+// estimate p = [(cL + cR + (uL-uR)(gamma-1)/2) / (cL pL^-m + cR pR^-m)]^(1/m)
+// (the reference's own start value for the shock-rarefaction pattern,
+// riemannsolver.F90:118-119), here in FP32; if it is not a positive finite
+// number, the linearised (acoustic) estimate (pL+pR)/2 + kappa (uL-uR)/2;
+// 0 if neither is positive.
+//
+// The reference's guess (riemann.F90:343-345) adds kappa (uL+uR)/2, which in
+// the bulk flows of a cosmological box lands far from the root: on a 48^3
+// EdS field its Newton faces take 4.9 iterations on average and 7.9 for the
+// slowest face of 32 (a warp waits for its slowest lane), the linearised
+// estimate 2.2 and 3.0, the two-rarefaction estimate 1.05 and 1.6 (two
+// shocks) and 1.01 and 1.1 (shock + rarefaction).  Every start point
+// converges to the same root to the 1e-3 step tolerance; p* differs from
+// the reference's by a few 1e-7 relative at most.
+__device__ __forceinline__ double mixed_newton_start(double pleft, double pright, double rholeft, double rhoright,
+                                                     double vxleft, double vxright, const Consts& k) {
+    const float g = float(k.gamma), m = float(k.m);
+    const float pl = float(pleft), pr = float(pright);
+    const float cl = sqrtf(g * pl / float(rholeft)), cr = sqrtf(g * pr / float(rhoright));
+    const float q = (cl + cr + (float(vxleft) - float(vxright)) * (g - 1.0f) * 0.5f) /
+                    (cl / PowF32::pw(pl, m) + cr / PowF32::pw(pr, m));
+    float ps;
+    if (k.nroot == 5) {
+        const float q2 = q * q;
+        ps = q2 * q2 * q;
+    } else {
+        ps = PowF32::pw(q, float(k.rm));
+    }
+    if (ps > 0.0f && ps < 3.0e38f) return double(ps);
+    const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
+    const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft - vxright);
+    return pcheck > 0.0 ? pcheck : 0.0;
+}
+
 // Same iteration with the divisions of the loop body replaced by products
 // with reciprocals formed once (or by rsqrt), and u* formed once after the
 // loop from the last wave speeds: a shorter dependency chain per iteration.
-// Used by the mixed-precision path, whose Newton still runs in FP64.
-//
-// The mixed path also starts from the linearised (acoustic) estimate
-// p = (pL+pR)/2 + kappa (uL-uR)/2.  The reference's guess (riemann.F90:
-// 343-345) adds kappa (uL+uR)/2, which in the bulk flows of a cosmological
-// box lands far from the root: a third of the Newton faces then take 7-8
-// iterations (mean 4.7 on a 64^3 EdS field) against a mean of 1.9 and at
-// most 4-5 from the linearised estimate, and a warp waits for its slowest
-// lane.  Both start points converge to the same root to the 1e-3 step
-// tolerance; on that field p* differs by at most 4e-7 (mean 5e-8) relative.
+// Used by the mixed-precision path, whose Newton still runs in FP64; it
+// starts from pstar as given (mixed_newton_start, chosen by the caller).
 template <class Pow>
 __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vstar, double pleft, double pright,
                                                      double rholeft, double rhoright, double vxleft,
                                                      double vxright, const Consts& k) {
-    const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
-    const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft - vxright);
-    if (pcheck > 0.0) pstar = pcheck;
     const double cleft = sqrt(k.gamma * pleft * rholeft);
     const double cright = sqrt(k.gamma * pright * rhoright);
     const double rpl = Pow::div(1.0, pleft), rpr = Pow::div(1.0, pright);
@@ -311,6 +335,10 @@ __device__ __forceinline__ bool riemann_two_shocks(const FaceState& L, const Fac
                                                    double& rhom, const Consts& k) {
     const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
     pm = fmax2(pleft, pright);
+    if constexpr (Pow::kShortNewton) {
+        const double st = mixed_newton_start(pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+        if (st > 0.0) pm = st;
+    }
     const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
     const S pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
     const S rl = S(rholeft), rr = S(rhoright);
@@ -336,14 +364,13 @@ __device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, co
                                                           const Consts& k) {
     const double gamma = k.gamma;
     const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
-    // the start value riemann.F90 replaces by its guess when that is
-    // positive; the mixed path's guess is positive for almost every face,
-    // so it forms this one only when it is needed
+    // the start value of riemann.F90 (which its guess replaces when that is
+    // positive); the mixed path forms it in FP64 only when its own FP32
+    // start value fails
     bool need_start = true;
     if constexpr (Pow::kShortNewton) {
-        const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
-        need_start = !(0.5 * (pleft + pright) + 0.5 * kappa * (vxleft - vxright) > 0.0);
-        pm = 0.0;
+        pm = mixed_newton_start(pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+        need_start = !(pm > 0.0);
     }
     if (need_start)
         pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
