@@ -106,7 +106,7 @@ template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
 struct SweepSmem {
     using R = typename Policy::R;
     static constexpr int kG = GRAV ? P * RING : 1;
-    double st[5][P * RING];     // state ring: p, rho, u, v, w
+    R st[5][P * RING];          // state ring: p, rho, u, v, w (FP32 copy in the mixed path)
     double sg[kG];              // gravity ring: g = -gforce of this sweep's axis
     R slg[kG];                  // ajside slope of g
     R sl[5][P * RING];          // ajside slopes
@@ -209,7 +209,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             }
             const int ix = L::idx(e, tp);
 #pragma unroll
-            for (int q = 0; q < 5; ++q) S.st[q][ix] = v[q];
+            for (int q = 0; q < 5; ++q) S.st[q][ix] = R(v[q]);
             if constexpr (GRAV) {
                 // g(ippm) = -gforce(d, ...) (ppmsolver.F90:108,230,358); the
                 // field never changes, so no save area is needed
@@ -478,7 +478,17 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 f2.u = S.rs[2][id1];
                 f2.v = S.rs[3][id1];
                 f2.w = S.rs[4][id1];
-                double p = S.st[0][id], rho = S.st[1][id], u = S.st[2][id], v = S.st[3][id], w = S.st[4][id];
+                // the cell's FP64 state: from the ring in the FP64 path; the
+                // mixed path keeps an FP32 ring and reads it again from
+                // global memory, which still holds it (only this thread
+                // writes cell d, below)
+                const long long g = base + stride * d;
+                double p, rho, u, v, w;
+                if constexpr (sizeof(R) == sizeof(double)) {
+                    p = S.st[0][id]; rho = S.st[1][id]; u = S.st[2][id]; v = S.st[3][id]; w = S.st[4][id];
+                } else {
+                    p = a.f[0][g]; rho = a.f[1][g]; u = a.f[2][g]; v = a.f[3][g]; w = a.f[4][g];
+                }
                 // total() with the natural component order (ppmsolver.F90:149,277,405)
                 double etot;
                 if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
@@ -487,7 +497,6 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 using DivD = typename Policy::DivD;
                 if constexpr (GRAV) integrate<true, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[id]);
                 else integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
-                const long long g = base + stride * d;
                 if (a.flags & kFlagExpand) {
                     // expand.F90:161-176 with the step-start snapshot
                     const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
