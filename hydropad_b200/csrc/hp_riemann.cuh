@@ -106,8 +106,9 @@ struct PowRootBase {
 
 // FP64 path: roots to a few ulp, IEEE division, the literal loop body.
 struct PowRoot : PowRootBase<2> {
-    static constexpr bool kShortNewton = false;  // literal riemann.F90 loop body
+    static constexpr bool kShortNewton = false;  // the reference's Newton start value
     __device__ __forceinline__ static double div(double a, double b) { return a / b; }
+    __device__ __forceinline__ static double div_loop(double a, double b) { return a / b; }
 };
 
 // Mixed path: the shortened Newton loop body, and divisions from the
@@ -217,11 +218,13 @@ __device__ __forceinline__ double mixed_newton_start(double pleft, double pright
     return pcheck > 0.0 ? pcheck : 0.0;
 }
 
-// Same iteration with the divisions of the loop body replaced by products
-// with reciprocals formed once (or by rsqrt), and u* formed once after the
-// loop from the last wave speeds: a shorter dependency chain per iteration.
-// Used by the mixed-precision path, whose Newton still runs in FP64; it
-// starts from pstar as given (mixed_newton_start, chosen by the caller).
+// riemann.F90:318-400 with the divisions of the loop body replaced by
+// products with reciprocals formed once (or by rsqrt), and u* formed once
+// after the loop from the last wave speeds: the same iterates up to a few
+// ulp, with a shorter dependency chain per iteration.  Both paths run it in
+// FP64 from pstar as given: the FP64 path from the reference's start value
+// (riemann_newton below) with IEEE divisions, the mixed path from
+// mixed_newton_start (chosen by the caller) with refined reciprocals.
 template <class Pow>
 __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vstar, double pleft, double pright,
                                                      double rholeft, double rhoright, double vxleft,
@@ -279,51 +282,13 @@ template <class Pow>
 __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, double pleft, double pright,
                                                double rholeft, double rhoright, double vxleft, double vxright,
                                                const Consts& k) {
-    if constexpr (Pow::kShortNewton)
-        return riemann_newton_short<Pow>(pstar, vstar, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
-    double err = 1.e10;
-    int nnewt = 0;
-    const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
-    const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft + vxright);
-    if (pcheck > 0.0) pstar = pcheck;
-    const double cleft = sqrt(k.gamma * pleft * rholeft);
-    const double cright = sqrt(k.gamma * pright * rhoright);
-    while (err > kTerr) {
-        nnewt = nnewt + 1;
-        if (nnewt > kNewtonMax) return false;
-        const double pstarold = pstar;
-        double a, b, vprimel, vprimer;
-        // pstup (:360,:368) is only consulted on the rarefaction side, so the
-        // power is evaluated there alone.
-        const double rl = pstar / pleft, rr = pstar / pright;
-        if (pstar >= pleft) {
-            a = cleft * sqrt(k.gf * pstar / pleft + k.m);
-            vprimel = -((a * a + cleft * cleft) / (2.0 * a * a * a));
-        } else {
-            double pw, pg;
-            Pow::pm_pgf(rl, pw, pg, k);
-            if ((1.0 - pw) == 0.0) a = cleft * sqrt(k.gf * pstar / pleft + k.m);
-            else a = k.m * cleft * (1.0 - pstar / pleft) / (1.0 - pw);
-            vprimel = -((1.0 / cleft) * pg);
-        }
-        if (pstar >= pright) {
-            b = cright * sqrt(k.gf * pstar / pright + k.m);
-            vprimer = (b * b + cright * cright) / (2.0 * b * b * b);
-        } else {
-            double pw, pg;
-            Pow::pm_pgf(rr, pw, pg, k);
-            if ((1.0 - pw) == 0.0) b = cright * sqrt(k.gf * pstar / pright + k.m);
-            else b = k.m * cright * (1.0 - pstar / pright) / (1.0 - pw);
-            vprimer = (1.0 / cright) * pg;
-        }
-        const double vstarl = vxleft - (pstar - pleft) / a;
-        const double vstarr = vxright + (pstar - pright) / b;
-        pstar = pstar - (vstarl - vstarr) / (vprimel - vprimer);
-        if (pstar <= 0.0) pstar = pstarold / 1000.0;
-        vstar = (pleft - pright + a * vxleft + b * vxright) / (a + b);
-        err = fabs(pstarold - pstar) / pstarold;
+    if constexpr (!Pow::kShortNewton) {
+        // the reference's start value (riemann.F90:343-345)
+        const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
+        const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft + vxright);
+        if (pcheck > 0.0) pstar = pcheck;
     }
-    return true;
+    return riemann_newton_short<Pow>(pstar, vstar, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
 }
 
 // Pattern 1: two shocks, riemannsolver.F90:73-109.  The Newton iteration
