@@ -229,10 +229,25 @@ template <class Pow>
 __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vstar, double pleft, double pright,
                                                      double rholeft, double rhoright, double vxleft,
                                                      double vxright, const Consts& k) {
-    const double cleft = sqrt(k.gamma * pleft * rholeft);
-    const double cright = sqrt(k.gamma * pright * rhoright);
-    const double rpl = Pow::div(1.0, pleft), rpr = Pow::div(1.0, pright);
-    const double rcl = Pow::div(1.0, cleft), rcr = Pow::div(1.0, cright);
+    // Lagrangian sound speeds C = sqrt(gamma p rho) and the reciprocals the
+    // loop multiplies by
+    double cleft, cright, rpl, rpr, rcl, rcr;
+    if constexpr (Pow::kShortNewton) {
+        const double c2l = k.gamma * pleft * rholeft, c2r = k.gamma * pright * rhoright;
+        rcl = rsqrt(c2l);
+        rcr = rsqrt(c2r);
+        cleft = c2l * rcl;
+        cright = c2r * rcr;
+        rpl = Pow::div_loop(1.0, pleft);
+        rpr = Pow::div_loop(1.0, pright);
+    } else {
+        cleft = sqrt(k.gamma * pleft * rholeft);
+        cright = sqrt(k.gamma * pright * rhoright);
+        rpl = Pow::div(1.0, pleft);
+        rpr = Pow::div(1.0, pright);
+        rcl = Pow::div(1.0, cleft);
+        rcr = Pow::div(1.0, cright);
+    }
     // only 1/a and 1/b enter the iteration; u* = (pL-pR + a uL + b uR)/(a+b)
     // is formed once at the end from them
     double ia = 0.0, ib = 0.0;
@@ -274,7 +289,7 @@ __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vsta
             break;
         }
     }
-    vstar = Pow::div((pleft - pright) * ia * ib + vxleft * ib + vxright * ia, ia + ib);
+    vstar = Pow::div_loop((pleft - pright) * ia * ib + vxleft * ib + vxright * ia, ia + ib);
     return ok;
 }
 
