@@ -108,19 +108,29 @@ def grf_eds(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float =
 
 def grf_eds_device(n: int, seed: int = 12345, a_start: float = 1.0 / 51.0, rms: float = 0.5,
                    spectral_index: float = -2.0, kc_frac: float = 1.0 / 8.0, temp_k: float = 100.0,
-                   rho_floor: float = 1e-2, device="cuda"):
+                   rho_floor: float = 1e-2, device="cuda", noise: str = "host"):
     """:func:`grf_eds` with the spectral work on the GPU.
 
-    The white noise is the same PCG64 draw as :func:`grf_eds` (generated on
-    the host, so a seed gives the same field on every path); the FFTs, the
+    ``noise="host"``: the white noise is the same PCG64 draw as
+    :func:`grf_eds` (generated on the host, so a seed gives the same field on
+    every path).  ``noise="device"``: a normal draw of the device's own
+    generator (Philox) seeded with ``seed`` -- the same recipe and the same
+    field for a given seed and device, a different realisation from the host
+    draw, and no host work (the serving engine's choice).  The FFTs, the
     power-spectrum filter and the linear velocities run on ``device`` in
     FP64.  Returns ``(p, rho, vx, vy, vz)`` as contiguous float64 device
     tensors in the device state layout: shape ``(n, n, n)`` indexed
     ``[z, y, x]`` (x fastest), no ghosts -- the input of
-    ``Hydro.attach_device``.  Agrees with :func:`grf_eds` to FFT rounding."""
+    ``Hydro.attach_device``.  With host noise it agrees with :func:`grf_eds`
+    to FFT rounding."""
     import torch
-    rng = np.random.Generator(np.random.PCG64(seed))
-    white = torch.from_numpy(rng.standard_normal((n, n, n))).to(device)  # indexed [x, y, z] like grf_eds
+    if noise == "device":
+        gen = torch.Generator(device=device)
+        gen.manual_seed(int(seed))
+        white = torch.randn((n, n, n), generator=gen, dtype=torch.float64, device=device)
+    else:
+        rng = np.random.Generator(np.random.PCG64(seed))
+        white = torch.from_numpy(rng.standard_normal((n, n, n))).to(device)  # indexed [x, y, z] like grf_eds
     wk = torch.fft.rfftn(white)
     del white
     f64 = dict(dtype=torch.float64, device=wk.device)

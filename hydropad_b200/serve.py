@@ -107,6 +107,9 @@ class ServeStats:
     wall: float = 0.0
     budget_bytes: int = 0              # HBM budget of one rank
     offered: float = 0.0               # offered load of the whole trace, cell-updates/s
+    create_s: float = 0.0              # host time in admission (allocation, initial conditions)
+    sync_s: float = 0.0                # host time waiting for the batch at completions
+    finish_s: float = 0.0              # host time in retirement (download of the results)
 
     def summary(self) -> dict:
         lat = np.array([c.latency for c in self.completed]) if self.completed else np.zeros(1)
@@ -126,6 +129,9 @@ class ServeStats:
             "peak_resident_gb": self.peak_resident_bytes / 1e9,
             "batch_steps": self.steps_launched,
             "makespan_s": t1 - t0,
+            "host_admission_s": self.create_s,
+            "host_sync_wait_s": self.sync_s,
+            "host_retire_s": self.finish_s,
         }
 
 
@@ -141,6 +147,9 @@ def merge_stats(parts) -> ServeStats:
         out.peak_resident_bytes = max(out.peak_resident_bytes, st.peak_resident_bytes)
         out.steps_launched += st.steps_launched
         out.wall = max(out.wall, st.wall)
+        out.create_s += st.create_s
+        out.sync_s += st.sync_s
+        out.finish_s += st.finish_s
     out.completed.sort(key=lambda c: c.rid)
     return out
 
@@ -183,8 +192,10 @@ class Scheduler:
                 if resident + need > self.budget:
                     break
                 req = queue.popleft()
+                tc = time.perf_counter()
                 box = eng.create(req)
                 eng.add(box)
+                st.create_s += time.perf_counter() - tc
                 resident += need
                 active.append(Member(req, box, req.steps, eng.now()))
             st.peak_resident_bytes = max(st.peak_resident_bytes, resident)
@@ -208,9 +219,13 @@ class Scheduler:
                 m.remaining -= k
             done = [m for m in active if m.remaining == 0]
             if done:
+                tc = time.perf_counter()
                 eng.sync()
+                st.sync_s += time.perf_counter() - tc
                 for m in done:
+                    tc = time.perf_counter()
                     res = eng.finish(m.box)
+                    st.finish_s += time.perf_counter() - tc
                     t = eng.now()
                     st.completed.append(Completed(m.req.rid, m.req.side, m.req.steps, m.req.arrival, m.admitted, t,
                                                   res if self.keep_results else None))
@@ -274,7 +289,7 @@ class GpuEngine:
             if req.side not in self.initial:
                 self.initial[req.side] = h.get_scalars()
         state = ics.grf_eds_device(req.side, seed=req.seed, spectral_index=req.spectral_index,
-                                   device=f"cuda:{self.device}")
+                                   device=f"cuda:{self.device}", noise="device")
         h.attach_device(*state)
         del state
         h.start_with_cfl()
@@ -334,7 +349,7 @@ def run_alone(req: Request, precision: str, tiles=None, device: int = 0):
     h = Hydro(GpuEngine.params(req.side), precision=precision, device=device)
     with h:
         h.attach_device(*ics.grf_eds_device(req.side, seed=req.seed, spectral_index=req.spectral_index,
-                                            device=f"cuda:{device}"))
+                                            device=f"cuda:{device}", noise="device"))
         if tiles is not None:
             h.set_tiles(*tiles)
         h.start_with_cfl()
