@@ -39,11 +39,17 @@ struct StepScalars {
 // ajside, ppm_functs.F90:167-181: limited slope of the middle cell.
 // Evaluated without a branch (the discarded quotient may be NaN), which keeps
 // the warp converged; the selected value is the reference's.
+//
+// The FP32 instantiations (mixed path) below use multiply-adds, reciprocals
+// and sign copies where the FP64 ones keep the reference's operations: the
+// same values to FP32 rounding.
 template <class R>
 __device__ __forceinline__ R ajside(R am1, R a, R ap1) {
     const R da = R(0.5) * (ap1 - am1);
     const R mn = fmin2(fmin2(fabs(da), R(2) * fabs(a - am1)), R(2) * fabs(ap1 - a));
-    const R v = mn * da / fabs(da);
+    R v;
+    if constexpr (sizeof(R) == sizeof(float)) v = copysignf(mn, da);  // da != 0 whenever it is selected
+    else v = mn * da / fabs(da);
     return ((ap1 - a) * (a - am1) > R(0)) ? v : R(0);
 }
 
@@ -52,8 +58,12 @@ __device__ __forceinline__ R ajside(R am1, R a, R ap1) {
 // assign gradleft in the reference; it contributes nothing new here.
 template <class R>
 __device__ __forceinline__ bool flat_pair(R left, R right, R mingradflat) {
-    const R g = fabs((right - left) / fmin2(right, left));
-    return (right * left != R(0)) && (g >= mingradflat);
+    if constexpr (sizeof(R) == sizeof(float)) {
+        return (right * left != 0.0f) && (fabsf(right - left) >= mingradflat * fabsf(fminf(right, left)));
+    } else {
+        const R g = fabs((right - left) / fmin2(right, left));
+        return (right * left != R(0)) && (g >= mingradflat);
+    }
 }
 
 // Second difference used by dda (dda.F90:198-199), centred on the middle cell.
@@ -76,8 +86,14 @@ template <class R>
 __device__ __forceinline__ Parabola<R> build_parabola(R q1, R q2, R q3, R dm, R d0, R dp, R flat,
                                                       bool steepen, R Dm, R Dp, R dx) {
     Parabola<R> P;
-    R ajl = q1 + R(0.5) * (q2 - q1) + (dm - d0) * R(kSixth);
-    R ajr = q2 + R(0.5) * (q3 - q2) + (d0 - dp) * R(kSixth);
+    R ajl, ajr;
+    if constexpr (sizeof(R) == sizeof(float)) {
+        ajl = fmaf(dm - d0, float(kSixth), fmaf(0.5f, q2 - q1, q1));
+        ajr = fmaf(d0 - dp, float(kSixth), fmaf(0.5f, q3 - q2, q2));
+    } else {
+        ajl = q1 + R(0.5) * (q2 - q1) + (dm - d0) * R(kSixth);
+        ajr = q2 + R(0.5) * (q3 - q2) + (d0 - dp) * R(kSixth);
+    }
     if (steepen) {
         R eta;
         R agrad = fabs(q3 - q1) - R(kC010) * fmin2(fabs(q3), fabs(q1));
@@ -102,12 +118,18 @@ __device__ __forceinline__ Parabola<R> build_parabola(R q1, R q2, R q3, R dm, R 
     } else if (d * a6 < -(d * d)) {
         ajr = R(3) * q2 - R(2) * ajl;
     }
-    ajl = flat * q2 + (R(1) - flat) * ajl;
-    ajr = flat * q2 + (R(1) - flat) * ajr;
+    if constexpr (sizeof(R) == sizeof(float)) {
+        ajl = fmaf(flat, q2 - ajl, ajl);
+        ajr = fmaf(flat, q2 - ajr, ajr);
+        P.a6 = fmaf(-3.0f, ajl + ajr, 6.0f * q2);
+    } else {
+        ajl = flat * q2 + (R(1) - flat) * ajl;
+        ajr = flat * q2 + (R(1) - flat) * ajr;
+        P.a6 = R(6) * (q2 - R(0.5) * (ajl + ajr));
+    }
     P.jl = ajl;
     P.jr = ajr;
     P.d = ajr - ajl;
-    P.a6 = R(6) * (q2 - R(0.5) * (ajl + ajr));
     return P;
 }
 
@@ -115,25 +137,48 @@ __device__ __forceinline__ Parabola<R> build_parabola(R q1, R q2, R q3, R dm, R 
 // (the same x serves every variable of the cell).
 template <class R>
 __device__ __forceinline__ R fl(const Parabola<R>& P, R x) {
-    return P.jr - R(0.5) * x * (P.d - (R(1) - R(2) * x * R(kThird)) * P.a6);
+    if constexpr (sizeof(R) == sizeof(float)) {
+        const float t = fmaf(-2.0f * float(kThird), x, 1.0f);
+        return fmaf(-0.5f * x, fmaf(-t, P.a6, P.d), P.jr);
+    } else {
+        return P.jr - R(0.5) * x * (P.d - (R(1) - R(2) * x * R(kThird)) * P.a6);
+    }
 }
 template <class R>
 __device__ __forceinline__ R fr(const Parabola<R>& P, R x) {
-    return P.jl + R(0.5) * x * (P.d + (R(1) - R(2) * x * R(kThird)) * P.a6);
+    if constexpr (sizeof(R) == sizeof(float)) {
+        const float t = fmaf(-2.0f * float(kThird), x, 1.0f);
+        return fmaf(0.5f * x, fmaf(t, P.a6, P.d), P.jl);
+    } else {
+        return P.jl + R(0.5) * x * (P.d + (R(1) - R(2) * x * R(kThird)) * P.a6);
+    }
 }
 
 // beta, ppm_functs.F90:129-144 (expanding-coordinate characteristic term).
 template <class R>
 __device__ __forceinline__ R beta(R ct, R ut, R uc, R pt, R pc, R gc, R sign, R dt, R at, R dat, R rat) {
-    R gvc = (-gc + dat * uc) * rat;
-    return -(sign * ((ut - uc) + sign * (pt - pc) / ct + sign * dt * (R(2) * dat * pc / (ct * at)) + dt * gvc)) /
-           (R(2) * ct);
+    if constexpr (sizeof(R) == sizeof(float)) {
+        // 1/ct is shared by every call of a face side; 1/at = rat
+        const float rct = 1.0f / ct;
+        const float gvc = (fmaf(dat, uc, -gc)) * rat;
+        const float in = fmaf(dt, gvc, fmaf(sign * dt, 2.0f * dat * pc * rct * rat, fmaf(sign * (pt - pc), rct, ut - uc)));
+        return -(sign * in) * (0.5f * rct);
+    } else {
+        R gvc = (-gc + dat * uc) * rat;
+        return -(sign * ((ut - uc) + sign * (pt - pc) / ct + sign * dt * (R(2) * dat * pc / (ct * at)) + dt * gvc)) /
+               (R(2) * ct);
+    }
 }
 
 // beta0, ppm_functs.F90:149-162.
 template <class R>
 __device__ __forceinline__ R beta0(R ct, R rhot, R rhoc, R pt, R pc, R dt, R at, R dat) {
-    return (pt - pc) / (ct * ct) + R(1) / rhot - R(1) / rhoc + (R(2) * dat * pc) / (at * ct * ct) * dt;
+    if constexpr (sizeof(R) == sizeof(float)) {
+        const float rct = 1.0f / ct, rct2 = rct * rct;
+        return fmaf(pt - pc, rct2, 1.0f / rhot - 1.0f / rhoc) + (2.0f * dat * pc) * (rct2 / at) * dt;
+    } else {
+        return (pt - pc) / (ct * ct) + R(1) / rhot - R(1) / rhoc + (R(2) * dat * pc) / (at * ct * ct) * dt;
+    }
 }
 
 struct FaceState {
