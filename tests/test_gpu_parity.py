@@ -184,3 +184,57 @@ def test_autotune_keeps_state():
     assert all(0 <= t < num_tiles() for t in tiles)
     for a, b in zip(before, after):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("shape", [(24, 16, 20), (16, 32, 12)])
+def test_evolve_fp64_non_cubic(oracle, shape):
+    """Non-cubic boxes (dx = 1/max(N), the pencils of each axis have their
+    own length): 6 steps within the FP64 gate of the oracle."""
+    rng = np.random.Generator(np.random.PCG64(31))
+    x, y, z = np.meshgrid(*[(np.arange(n) + 0.5) / n for n in shape], indexing="ij")
+    rho = 1.0 + 0.4 * np.sin(2 * np.pi * x) * np.cos(2 * np.pi * y) + 0.1 * rng.random(shape)
+    p = 0.6 + 0.3 * np.cos(2 * np.pi * z) + 0.1 * rng.random(shape)
+    vel = [0.3 * np.sin(2 * np.pi * (x + 2 * y + 3 * z + q)) for q in range(3)]
+    state = [np.asfortranarray(np.pad(a, NB, mode="wrap")) for a in (p, rho, *vel)]
+    prm = params_for(shape)
+    st = oracle.OracleState(*state)
+    s = oracle.make_scalars(prm)
+    oracle_first_dt(oracle, st, s)
+    with _hydro(prm) as h:
+        h.attach_state(*state)
+        _copy_scalars(h, s)
+        h.evolve(6, graph=True)
+        out = h.download()
+    assert st.evolve(s, 6) == 0
+    _assert_fields(out, st.f, FP64_TOL, f"non-cubic {shape}")
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_invalid_state_is_reported(prec):
+    """A non-physical input (one cell with negative density) is caught by the
+    device status word: the step returns an error instead of silently
+    producing NaN, and the context stays usable."""
+    from hydropad_b200._lib import HydroError
+    n = 16
+    state = [a.copy(order="F") for a in sod_state(n)]
+    state[1][NB + 5, NB + 5, NB + 5] = -0.5
+    prm = params_for((n, n, n))
+    with _hydro(prm, prec) as h:
+        s0 = h.get_scalars()
+        h.attach_state(*state)
+        h.start_with_cfl()
+        with pytest.raises(HydroError, match="NAN|NEGATIVE"):
+            h.evolve(1)
+        # the context still runs a valid state once its clock is reset
+        h.attach_state(*sod_state(n))
+        h.set_scalars(s0)
+        h.start_with_cfl()
+        h.evolve(2)
+        again = h.download()
+    with _hydro(prm, prec) as h:
+        h.attach_state(*sod_state(n))
+        h.start_with_cfl()
+        h.evolve(2)
+        fresh = h.download()
+    for a, b in zip(again, fresh):
+        assert np.array_equal(a, b)
