@@ -91,49 +91,64 @@ int copy_ctl_to_host(hp_ctx* x) {
     return HP_OK;
 }
 
-// Ghosted Fortran host array <-> dense device interior.
-cudaMemcpy3DParms host_dev_parms(const double* host, double* dev, const hp_ctx* x, int nxg, int nyg, int nb,
-                                 bool to_device) {
-    cudaMemcpy3DParms prm;
-    memset(&prm, 0, sizeof prm);
-    cudaPitchedPtr hp_ = make_cudaPitchedPtr((void*)host, (size_t)nxg * sizeof(double), (size_t)nxg, (size_t)nyg);
-    cudaPitchedPtr dp_ = make_cudaPitchedPtr((void*)dev, (size_t)x->box.nx * sizeof(double), (size_t)x->box.nx,
-                                             (size_t)x->box.ny);
-    cudaPos hpos = make_cudaPos((size_t)nb * sizeof(double), (size_t)nb, (size_t)nb);
-    cudaPos dpos = make_cudaPos(0, 0, 0);
-    if (to_device) {
-        prm.srcPtr = hp_; prm.srcPos = hpos; prm.dstPtr = dp_; prm.dstPos = dpos;
-        prm.kind = cudaMemcpyHostToDevice;
-    } else {
-        prm.srcPtr = dp_; prm.srcPos = dpos; prm.dstPtr = hp_; prm.dstPos = hpos;
-        prm.kind = cudaMemcpyDeviceToHost;
-    }
-    prm.extent = make_cudaExtent((size_t)x->box.nx * sizeof(double), (size_t)x->box.ny, (size_t)x->box.nz);
-    return prm;
+// Ghosted Fortran host array <-> dense device field.  The host array is
+// moved in contiguous runs of whole (nxg x nyg) planes through a device
+// staging buffer (full-speed DMA, unlike a pitched 3-D copy of the
+// interior); a kernel extracts the interior on the way in and writes the
+// interior plus its periodic ghost layers on the way out, so the host
+// array comes back with its ghosts filled (exchange_mesh.F90:23-41 for one
+// rank).  All on the context's stream.
+constexpr size_t kStageBytes = size_t(32) << 20;
+
+int ensure_stage(hp_ctx* x, size_t plane_bytes) {
+    size_t want = plane_bytes > kStageBytes ? plane_bytes : (kStageBytes / plane_bytes) * plane_bytes;
+    if (x->stage && x->stage_bytes >= want) return HP_OK;
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    cudaFree(x->stage);
+    x->stage = nullptr;
+    x->stage_bytes = 0;
+    HP_CUDA(cudaMalloc(&x->stage, want));
+    x->stage_bytes = want;
+    return HP_OK;
 }
 
-// Periodic ghost layers of one host array (exchange_mesh.F90 with one rank).
-void fill_ghosts(double* a, int nx, int ny, int nz, int nb) {
-#define IX(i, j, k) ((size_t)(i) + (size_t)nx * ((size_t)(j) + (size_t)ny * (size_t)(k)))
-    for (int k = 0; k < nb; ++k)
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < nx; ++i) {
-                a[IX(i, j, k)] = a[IX(i, j, nz - 2 * nb + k)];
-                a[IX(i, j, nz - nb + k)] = a[IX(i, j, k + nb)];
-            }
-    for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < nb; ++j)
-            for (int i = 0; i < nx; ++i) {
-                a[IX(i, j, k)] = a[IX(i, ny - 2 * nb + j, k)];
-                a[IX(i, ny - nb + j, k)] = a[IX(i, j + nb, k)];
-            }
-    for (int k = 0; k < nz; ++k)
-        for (int j = 0; j < ny; ++j)
-            for (int i = 0; i < nb; ++i) {
-                a[IX(i, j, k)] = a[IX(nx - 2 * nb + i, j, k)];
-                a[IX(nx - nb + i, j, k)] = a[IX(i + nb, j, k)];
-            }
-#undef IX
+int upload_field(hp_ctx* x, const double* host, double* f, int nb) {
+    const int nx = x->box.nx, ny = x->box.ny, nz = x->box.nz;
+    if (nb == 0)
+        return cuda_fail(cudaMemcpyAsync(f, host, (size_t)nx * ny * nz * sizeof(double), cudaMemcpyHostToDevice,
+                                         x->stream));
+    const size_t plane = (size_t)(nx + 2 * nb) * (ny + 2 * nb);
+    int rc = ensure_stage(x, plane * sizeof(double));
+    if (rc != HP_OK) return rc;
+    const int per = (int)(x->stage_bytes / (plane * sizeof(double)));
+    for (int zg = nb; zg < nb + nz; zg += per) {
+        const int k = per < nb + nz - zg ? per : nb + nz - zg;
+        HP_CUDA(cudaMemcpyAsync(x->stage, host + (size_t)zg * plane, (size_t)k * plane * sizeof(double),
+                                cudaMemcpyHostToDevice, x->stream));
+        if (hp::launch_planes_to_field(x->stage, f, nx, ny, nb, zg - nb, k, x->stream) < 0) return HP_ERR_CUDA;
+        x->launches += 1;
+    }
+    return HP_OK;
+}
+
+int download_field(hp_ctx* x, const double* f, double* host, int nb) {
+    const int nx = x->box.nx, ny = x->box.ny, nz = x->box.nz;
+    if (nb == 0)
+        return cuda_fail(cudaMemcpyAsync(host, f, (size_t)nx * ny * nz * sizeof(double), cudaMemcpyDeviceToHost,
+                                         x->stream));
+    const int nzg = nz + 2 * nb;
+    const size_t plane = (size_t)(nx + 2 * nb) * (ny + 2 * nb);
+    int rc = ensure_stage(x, plane * sizeof(double));
+    if (rc != HP_OK) return rc;
+    const int per = (int)(x->stage_bytes / (plane * sizeof(double)));
+    for (int zg = 0; zg < nzg; zg += per) {
+        const int k = per < nzg - zg ? per : nzg - zg;
+        if (hp::launch_field_to_planes(f, x->stage, nx, ny, nz, nb, zg, k, x->stream) < 0) return HP_ERR_CUDA;
+        x->launches += 1;
+        HP_CUDA(cudaMemcpyAsync(host + (size_t)zg * plane, x->stage, (size_t)k * plane * sizeof(double),
+                                cudaMemcpyDeviceToHost, x->stream));
+    }
+    return HP_OK;
 }
 
 // One fused sweep on the resident state.
@@ -332,6 +347,7 @@ int hp_finalize(hp_ctx* x) {
     for (int q = 0; q < 5; ++q) cudaFree(x->box.f[q]);
     for (int q = 0; q < 4; ++q) cudaFree(x->box.snap[q]);
     cudaFree(x->box.peak);
+    cudaFree(x->stage);
     for (int q = 0; q < 3; ++q) cudaFree(x->box.g[q]);
     cudaFree(x->box.ctl);
     if (x->ctl_pinned) cudaFreeHost(x->ctl_pinned);
@@ -383,8 +399,8 @@ int hp_attach_state(hp_ctx* x, const double* p3d, const double* rho3d, const dou
     x->host_g = gforce;
     const double* src[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
     for (int q = 0; q < 5; ++q) {
-        cudaMemcpy3DParms prm = host_dev_parms(src[q], x->box.f[q], x, nx, ny, nbound, true);
-        HP_CUDA(cudaMemcpy3DAsync(&prm, x->stream));
+        const int rc = upload_field(x, src[q], x->box.f[q], nbound);
+        if (rc != HP_OK) return rc;
         x->host[q] = src[q];
     }
     x->hnx = nx; x->hny = ny; x->hnz = nz; x->hnb = nbound;
@@ -427,12 +443,10 @@ int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, doubl
     HP_CUDA(cudaSetDevice(x->dev));
     double* dst[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
     for (int q = 0; q < 5; ++q) {
-        cudaMemcpy3DParms prm = host_dev_parms(dst[q], x->box.f[q], x, nx, ny, nbound, false);
-        HP_CUDA(cudaMemcpy3DAsync(&prm, x->stream));
+        const int rc = download_field(x, x->box.f[q], dst[q], nbound);
+        if (rc != HP_OK) return rc;
     }
     HP_CUDA(cudaStreamSynchronize(x->stream));
-    if (nbound > 0)
-        for (int q = 0; q < 5; ++q) fill_ghosts(dst[q], nx, ny, nz, nbound);
     return HP_OK;
 }
 

@@ -22,6 +22,8 @@ struct hp_ctx {
     cudaGraphExec_t graph[6][3];
     int graph_kernels[6][3];
     long long launches;
+    double* stage;            // device staging of host-layout planes (host transfers), or null
+    size_t stage_bytes;
 };
 
 namespace hp {

@@ -167,6 +167,50 @@ int launch_deinterleave3(const double* in, double* g0, double* g1, double* g2, l
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 
+// Host-layout planes <-> dense device field.  A ghosted host array is
+// (nxg, nyg, nzg) with nb ghost layers per side, x fastest; `stage` holds
+// the ghosted planes zg0 .. zg0+nplanes-1 of it contiguously.
+__global__ void planes_to_field_kernel(const double* __restrict__ stage, double* __restrict__ f, int nx, int ny,
+                                       int nb, int zf0, int nplanes) {
+    const int nxg = nx + 2 * nb, nyg = ny + 2 * nb;
+    const long long n = (long long)nx * ny * nplanes;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nx);
+        const int j = (int)((t / nx) % ny);
+        const int kz = (int)(t / ((long long)nx * ny));
+        f[i + (long long)nx * (j + (long long)ny * (zf0 + kz))] =
+            stage[(i + nb) + (long long)nxg * ((j + nb) + (long long)nyg * kz)];
+    }
+}
+
+// The ghosted planes zg0 .. zg0+nplanes-1 of a field, periodic ghosts
+// included (the exchange_mesh fill of a single rank, exchange_mesh.F90:23-41).
+__global__ void field_to_planes_kernel(const double* __restrict__ f, double* __restrict__ stage, int nx, int ny,
+                                       int nz, int nb, int zg0, int nplanes) {
+    const int nxg = nx + 2 * nb, nyg = ny + 2 * nb;
+    const long long n = (long long)nxg * nyg * nplanes;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int ig = (int)(t % nxg);
+        const int jg = (int)((t / nxg) % nyg);
+        const int kz = (int)(t / ((long long)nxg * nyg));
+        const int i = ((ig - nb) % nx + nx) % nx;
+        const int j = ((jg - nb) % ny + ny) % ny;
+        const int k = ((zg0 + kz - nb) % nz + nz) % nz;
+        stage[t] = f[i + (long long)nx * (j + (long long)ny * k)];
+    }
+}
+
+int launch_planes_to_field(const double* stage, double* f, int nx, int ny, int nb, int zf0, int nplanes,
+                           cudaStream_t st) {
+    planes_to_field_kernel<<<1184, 256, 0, st>>>(stage, f, nx, ny, nb, zf0, nplanes);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+int launch_field_to_planes(const double* f, double* stage, int nx, int ny, int nz, int nb, int zg0, int nplanes,
+                           cudaStream_t st) {
+    field_to_planes_kernel<<<1184, 256, 0, st>>>(f, stage, nx, ny, nz, nb, zg0, nplanes);
+    return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
+}
+
 // FP64 -> FP32, round to nearest even (Fortran REAL() of a REAL(8), the
 // conversion write_var_mpi.F90:55 applies before writing).
 __global__ void to_f32_kernel(const double* __restrict__ in, float* __restrict__ out, long long n) {

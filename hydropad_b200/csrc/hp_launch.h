@@ -43,6 +43,13 @@ int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st);
 int launch_timedet_batch(DevCtl* const* ctls, int n, cudaStream_t st);
 // in = (3, n) interleaved (gforce(3,nx,ny,nz) interior) -> g0, g1, g2.
 int launch_deinterleave3(const double* in, double* g0, double* g1, double* g2, long long n, cudaStream_t st);
+// Ghosted host-layout planes (contiguous, staged on the device) <-> a dense
+// field: the interior of planes zf0.. of the field from `stage`, or the
+// ghosted planes zg0.. (periodic ghosts filled) of the field into `stage`.
+int launch_planes_to_field(const double* stage, double* f, int nx, int ny, int nb, int zf0, int nplanes,
+                           cudaStream_t st);
+int launch_field_to_planes(const double* f, double* stage, int nx, int ny, int nz, int nb, int zg0, int nplanes,
+                           cudaStream_t st);
 // out[i] = (float)in[i], round to nearest even.
 int launch_to_f32(const double* in, float* out, long long n, cudaStream_t st);
 // out[i] = status word of ctls[i], which is cleared.

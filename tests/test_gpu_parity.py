@@ -238,3 +238,26 @@ def test_invalid_state_is_reported(prec):
         fresh = h.download()
     for a, b in zip(again, fresh):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (24, 16, 20)])
+def test_host_transfers_round_trip(shape):
+    """attach_state / download / sync_to_host move whole ghosted planes
+    through a device staging buffer: the interior comes back unchanged and
+    the ghost layers hold the periodic copies (exchange_mesh for one rank)."""
+    rng = np.random.Generator(np.random.PCG64(5))
+    arrs = [np.asfortranarray(np.pad(1.0 + rng.random(shape), NB, mode="wrap")) for _ in range(5)]
+    for a in arrs:  # junk in the ghosts: they must not be read
+        a[:NB] = -7.0
+    with _hydro(params_for(shape)) as h:
+        host = h.attach_state(*arrs)
+        out = h.download()
+        synced = h.sync_to_host()
+        dense = h.download(nbound=0)
+    for a, o, s_, d in zip(arrs, out, synced, dense):
+        inner = interior(a)
+        assert np.array_equal(interior(o), inner)
+        assert np.array_equal(o, np.pad(inner, NB, mode="wrap"))
+        assert np.array_equal(s_, o)
+        assert np.array_equal(d, inner)
+    assert all(s_ is hh for s_, hh in zip(synced, host))
