@@ -261,3 +261,46 @@ def test_host_transfers_round_trip(shape):
         assert np.array_equal(s_, o)
         assert np.array_equal(d, inner)
     assert all(s_ is hh for s_, hh in zip(synced, host))
+
+
+def test_config1_sod64(oracle):
+    """The Sod configuration at its full size: 64^3, cour 0.8, 100 steps
+    with the reference's nrot schedule, against the oracle after 10 and
+    after 100 steps (the FP64 gate both times)."""
+    n = 64
+    state = sod_state(n, axis=0)
+    prm = params_for((n, n, n))
+    st = oracle.OracleState(*state)
+    s = oracle.make_scalars(prm)
+    oracle_first_dt(oracle, st, s)
+    with _hydro(prm) as h:
+        h.attach_state(*state)
+        _copy_scalars(h, s)
+        h.evolve(10, graph=True)
+        out10 = h.download()
+        h.evolve(90, graph=True)
+        out100 = h.download()
+        g = h.get_scalars()
+    assert st.evolve(s, 10) == 0
+    _assert_fields(out10, st.f, FP64_TOL, "Sod 64^3, 10 steps")
+    assert st.evolve(s, 90) == 0
+    _assert_fields(out100, st.f, FP64_TOL, "Sod 64^3, 100 steps")
+    assert abs(g.t - s.t) <= 1e-12 * s.t
+
+
+def test_config2_eds256_fp64_two_steps(oracle):
+    """The cosmological configuration at its full size (256^3): two steps of
+    the FP64 path against the oracle (parity at the size the bench runs)."""
+    n = 256
+    state = grf_state(n, seed=12345)
+    prm = params_for((n, n, n), cosmo=True)
+    st = oracle.OracleState(*state)
+    s = oracle.make_scalars(prm)
+    oracle_first_dt(oracle, st, s)
+    with _hydro(prm) as h:
+        h.attach_state(*state)
+        _copy_scalars(h, s)
+        h.evolve(2, graph=True)
+        out = h.download()
+    assert st.evolve(s, 2) == 0
+    _assert_fields(out, st.f, FP64_TOL, "EdS 256^3, 2 steps")
