@@ -14,6 +14,7 @@ HP_OK = 0
 HP_ERR = {
     -1: "HP_ERR_ARG", -2: "HP_ERR_CUDA", -3: "HP_ERR_OOM", -4: "HP_ERR_NEWTON", -5: "HP_ERR_NAN",
     -6: "HP_ERR_NEGATIVE_STATE", -7: "HP_ERR_NOT_ATTACHED", -8: "HP_ERR_STATE_MISMATCH", -9: "HP_ERR_NO_DEVICE",
+    -10: "HP_ERR_UNSUPPORTED",
 }
 HP_PREC_FP64 = 0
 HP_PREC_MIXED = 1
@@ -52,6 +53,8 @@ EXPORTS = (
     "hp_synchronize", "hp_stream", "hp_device_fields", "hp_strerror", "hp_launch_count", "hp_set_tiles",
     "hp_get_tiles", "hp_autotune", "hp_ppmsolver_noalloc", "hp_attach_device_state",
     "hp_write_var", "hp_evolve_async", "hp_attach_device_gforce", "hp_num_tiles",
+    "hp_slab_init", "hp_slab_get_edges", "hp_slab_set_halos", "hp_step_axis", "hp_step_sweep",
+    "hp_step_velmax", "hp_step_finish",
     "hp_batch_create", "hp_batch_destroy", "hp_batch_add", "hp_batch_remove", "hp_batch_size",
     "hp_batch_step", "hp_batch_synchronize", "hp_batch_member", "hp_batch_set_tiles", "hp_batch_get_tiles",
     "hp_batch_autotune", "hp_batch_stream", "hp_batch_launch_count",
@@ -81,6 +84,13 @@ def lib():
     L.hp_attach_device_state.argtypes = [cp, cp, cp, cp, cp, cp]
     L.hp_write_var.argtypes = [cp, C.c_char_p, C.c_int]
     L.hp_num_tiles.argtypes = []
+    L.hp_slab_init.argtypes = [cp, C.c_int, C.c_int]
+    L.hp_slab_get_edges.argtypes = [cp, cp, cp]
+    L.hp_slab_set_halos.argtypes = [cp, cp, cp]
+    L.hp_step_axis.argtypes = [cp, C.c_int]
+    L.hp_step_sweep.argtypes = [cp, C.c_int]
+    L.hp_step_velmax.argtypes = [cp, dp]
+    L.hp_step_finish.argtypes = [cp, C.c_double]
     L.hp_attach_device_gforce.argtypes = [cp, cp, cp, cp]
     L.hp_sync_to_host.argtypes = [cp]
     L.hp_download_state.argtypes = [cp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int]

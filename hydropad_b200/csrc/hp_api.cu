@@ -154,8 +154,13 @@ int download_field(hp_ctx* x, const double* f, double* host, int nb) {
 // One fused sweep on the resident state.
 int do_sweep(hp_ctx* x, int axis, int flags) {
     const int bslot = (int)(x->sweep_count % 3);
-    int n = hp::launch_peak_prepass(x->box, axis, bslot, x->stream);
-    if (n < 0) return HP_ERR_CUDA;
+    int n = 0;
+    if (x->slab && axis == 2) {
+        flags |= hp::kFlagZHalo;  // no pre-pass: its transposed gather would cross slabs
+    } else {
+        n = hp::launch_peak_prepass(x->box, axis, bslot, x->stream);
+        if (n < 0) return HP_ERR_CUDA;
+    }
     x->launches += n;
     n = hp::launch_sweep(x->box, axis, x->tile[axis], bslot, flags, x->prm.precision, x->stream);
     if (n < 0) return HP_ERR_CUDA;
@@ -244,6 +249,7 @@ const char* hp_strerror(int code) {
         case HP_ERR_NOT_ATTACHED: return "no state attached";
         case HP_ERR_STATE_MISMATCH: return "host arrays are not the attached state";
         case HP_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
+        case HP_ERR_UNSUPPORTED: return "not supported by this build (the density-peak fix across z slabs)";
     }
     return "unknown error";
 }
@@ -348,6 +354,8 @@ int hp_finalize(hp_ctx* x) {
     for (int q = 0; q < 4; ++q) cudaFree(x->box.snap[q]);
     cudaFree(x->box.peak);
     cudaFree(x->stage);
+    cudaFree(x->box.zlo);
+    cudaFree(x->box.zhi);
     for (int q = 0; q < 3; ++q) cudaFree(x->box.g[q]);
     cudaFree(x->box.ctl);
     if (x->ctl_pinned) cudaFreeHost(x->ctl_pinned);
@@ -562,7 +570,7 @@ int hp_ppmsolver(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, double* vy
 }
 
 int hp_ppm_lxlylz(hp_ctx* x, int nrot) {
-    if (!x || nrot < 1 || nrot > 6) return HP_ERR_ARG;
+    if (!x || nrot < 1 || nrot > 6 || x->slab) return HP_ERR_ARG;
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     HP_CUDA(cudaSetDevice(x->dev));
     for (int s = 0; s < 3; ++s) {
@@ -597,7 +605,7 @@ int hp_timedet(hp_ctx* x, double velmax) {
 }
 
 int hp_evolve_async(hp_ctx* x, int nsteps, int use_graph) {
-    if (!x || nsteps < 0) return HP_ERR_ARG;
+    if (!x || nsteps < 0 || x->slab) return HP_ERR_ARG;  // a slab steps through hp_step_*
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     HP_CUDA(cudaSetDevice(x->dev));
     for (int it = 0; it < nsteps; ++it) {
@@ -731,6 +739,96 @@ int hp_autotune(hp_ctx* x, int reps) {
     if (e1) cudaEventDestroy(e1);
     if (rc != HP_OK) return rc;
     return hp_set_tiles(x, pick[0], pick[1], pick[2]);
+}
+
+int hp_slab_init(hp_ctx* x, int nz_global, int z0) {
+    if (!x || x->slab) return HP_ERR_ARG;
+    const int nz = x->box.nz;
+    if (nz < 4 || z0 < 0 || nz_global < nz || z0 + nz > nz_global) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    const size_t plane = (size_t)x->box.nx * x->box.ny;
+    int rc = cuda_fail(cudaMalloc(&x->box.zlo, 5 * 4 * plane * sizeof(double)));
+    if (rc == HP_OK) rc = cuda_fail(cudaMalloc(&x->box.zhi, 5 * 3 * plane * sizeof(double)));
+    if (rc != HP_OK) {
+        cudaFree(x->box.zlo);
+        cudaFree(x->box.zhi);
+        x->box.zlo = x->box.zhi = nullptr;
+        return rc;
+    }
+    // dx of the whole box (initialize_parameters.F90:23): 1/max(ngridx, ngridy, nz_global)
+    const int nmax = x->box.nx > x->box.ny ? (x->box.nx > nz_global ? x->box.nx : nz_global)
+                                           : (x->box.ny > nz_global ? x->box.ny : nz_global);
+    x->box.k.dx = 1.0 / (double)nmax;
+    x->box.k.rdx = 1.0 / x->box.k.dx;
+    if ((rc = copy_ctl_to_host(x)) != HP_OK) return rc;
+    x->ctl_pinned->dx = x->box.k.dx;
+    if ((rc = copy_ctl_to_device(x)) != HP_OK) return rc;
+    drop_graphs(x);
+    x->slab = 1;
+    x->nz_global = nz_global;
+    x->z0 = z0;
+    return HP_OK;
+}
+
+int hp_slab_get_edges(hp_ctx* x, double* top4, double* bottom3) {
+    if (!x || !x->slab || !top4 || !bottom3) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    const size_t plane = (size_t)x->box.nx * x->box.ny;
+    const size_t nz = (size_t)x->box.nz;
+    for (int q = 0; q < 5; ++q) {
+        HP_CUDA(cudaMemcpyAsync(top4 + q * 4 * plane, x->box.f[q] + (nz - 4) * plane, 4 * plane * sizeof(double),
+                                cudaMemcpyDeviceToDevice, x->stream));
+        HP_CUDA(cudaMemcpyAsync(bottom3 + q * 3 * plane, x->box.f[q], 3 * plane * sizeof(double),
+                                cudaMemcpyDeviceToDevice, x->stream));
+    }
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    return HP_OK;
+}
+
+int hp_slab_set_halos(hp_ctx* x, const double* lower4, const double* upper3) {
+    if (!x || !x->slab || !lower4 || !upper3) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    const size_t plane = (size_t)x->box.nx * x->box.ny;
+    HP_CUDA(cudaMemcpyAsync(x->box.zlo, lower4, 5 * 4 * plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                            x->stream));
+    HP_CUDA(cudaMemcpyAsync(x->box.zhi, upper3, 5 * 3 * plane * sizeof(double), cudaMemcpyDeviceToDevice,
+                            x->stream));
+    return HP_OK;
+}
+
+int hp_step_axis(hp_ctx* x, int s) {
+    if (!x || s < 0 || s > 2) return HP_ERR_ARG;
+    return hp::kSweepOrder[hp::nrot_of_step(x->nstep_host) - 1][s];
+}
+
+int hp_step_sweep(hp_ctx* x, int s) {
+    if (!x || s < 0 || s > 2) return HP_ERR_ARG;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    HP_CUDA(cudaSetDevice(x->dev));
+    return do_sweep(x, hp::kSweepOrder[hp::nrot_of_step(x->nstep_host) - 1][s], hp::step_flags(x->prm, s));
+}
+
+int hp_step_velmax(hp_ctx* x, double* velmax) {
+    if (!x || !velmax) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    unsigned long long bits = 0;
+    HP_CUDA(cudaMemcpyAsync(&bits, &x->box.ctl->velmax_key, sizeof bits, cudaMemcpyDeviceToHost, x->stream));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    memcpy(velmax, &bits, sizeof(double));
+    return HP_OK;
+}
+
+int hp_step_finish(hp_ctx* x, double velmax) {
+    if (!x) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    unsigned long long bits;
+    memcpy(&bits, &velmax, sizeof bits);
+    HP_CUDA(cudaMemcpyAsync(&x->box.ctl->velmax_key, &bits, sizeof bits, cudaMemcpyHostToDevice, x->stream));
+    if (hp::launch_timedet(x->box, 1, x->stream) < 0) return HP_ERR_CUDA;
+    x->launches += 1;
+    x->nstep_host += 1;
+    return hp_synchronize(x);
 }
 
 int hp_device_fields(hp_ctx* x, double** p, double** rho, double** vx, double** vy, double** vz) {

@@ -288,6 +288,7 @@ int hp_batch_add(hp_batch* b, hp_ctx* x) {
     if ((int)b->members.size() >= b->cap) return HP_ERR_ARG;
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     if (x->box.g[0]) return HP_ERR_ARG;  // the batched sweeps carry no gravity source
+    if (x->slab) return HP_ERR_ARG;      // nor the halos of a z slab
     if (std::find(b->members.begin(), b->members.end(), x) != b->members.end()) return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(b->dev));
     HP_CUDA(cudaStreamSynchronize(x->stream));  // the member's own work is finished

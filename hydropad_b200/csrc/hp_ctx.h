@@ -24,6 +24,8 @@ struct hp_ctx {
     long long launches;
     double* stage;            // device staging of host-layout planes (host transfers), or null
     size_t stage_bytes;
+    int slab;                 // 1: a z slab of a larger periodic box (hp_slab_init)
+    int nz_global, z0;
 };
 
 namespace hp {
@@ -35,6 +37,7 @@ inline int status_error(unsigned st) {
     if (st & kStatNewton) return HP_ERR_NEWTON;
     if (st & kStatNaN) return HP_ERR_NAN;
     if (st & kStatNegative) return HP_ERR_NEGATIVE_STATE;
+    if (st & kStatUnsupported) return HP_ERR_UNSUPPORTED;
     return HP_OK;
 }
 

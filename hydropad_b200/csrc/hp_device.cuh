@@ -12,6 +12,7 @@ enum : unsigned {
     kStatNewton = 1u,    // Newton for p* exceeded 100 iterations
     kStatNaN = 2u,       // NaN in an updated cell
     kStatNegative = 4u,  // rho <= 0 or p <= 0 in an updated cell
+    kStatUnsupported = 8u,  // a case the sweep cannot take (the density-peak fix across z slabs)
 };
 
 // Sweep flags.
@@ -21,6 +22,7 @@ enum : int {
     kFlagSpeed = 4,        // accumulate velmax of the updated cells
     kFlagResetSpeed = 8,   // zero the velmax accumulator (first sweep of a step)
     kFlagExpandZeroOld = 16,  // expand with vxold = pold3d = 0 (as alloc_arrays.F90:178-181 leaves them)
+    kFlagZHalo = 32,       // z sweep of a slab: the cells beyond its ends come from halo planes
 };
 
 // Time scalars + bookkeeping, one per box, in device memory so that a whole

@@ -13,6 +13,8 @@ struct Box {
     double* snap[4];   // step-start p, vx, vy, vz (cosmo expand), or null
     double* peak;      // density-peak scratch for y/z sweeps (nx*ny*nz), or null
     double* g[3];      // gforce components x, y, z (dense, natural layout), or null: gravity off
+    double* zlo;       // slab of a z-split box: 4 halo planes below, [p,rho,vx,vy,vz][4][nx*ny], or null
+    double* zhi;       // 3 halo planes above, [5][3][nx*ny], or null
     DevCtl* ctl;       // device control block
     Consts k;
     int nx, ny, nz;

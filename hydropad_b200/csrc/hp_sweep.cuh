@@ -47,6 +47,10 @@ struct SweepArgs {
     double* snap[4];       // step-start p, vx, vy, vz (natural order) for expand
     const double* peak;    // per-face density-peak values for y/z sweeps (may be null)
     const double* g;       // gforce component along this sweep (natural layout), or null: gravity off
+    // z sweep of a slab (kFlagZHalo): the 4 planes below and the 3 planes
+    // above the slab, [field][plane][nx*ny] in the sweep's field order
+    const double* zlo[5];
+    const double* zhi[5];
     DevCtl* ctl;
     Consts k;
     int nx, ny, nz;
@@ -184,7 +188,14 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             // original value (and the save area may not be written yet when
             // the pencil is shorter than one iteration).
             const bool from_save = e >= N && (e + 4) / T > (e - N + 8) / T;
-            if (from_save) {
+            const bool from_halo = AXIS == 2 && (a.flags & kFlagZHalo) && (e < 0 || e >= N);
+            if (from_halo) {
+                // a z slab's neighbours: planes -4..-1 below, N..N+2 above
+                const long long plane = (long long)a.nx * a.ny;
+                const long long off = (e < 0 ? (long long)(e + 4) : (long long)(e - N)) * plane + pid;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) v[q] = (e < 0 ? a.zlo[q] : a.zhi[q])[off];
+            } else if (from_save) {
 #pragma unroll
                 for (int q = 0; q < 5; ++q) v[q] = S.sv[q][(e - N) * P + tp];
             } else {
@@ -439,7 +450,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                     pattern, left, rgt, out, k, sc))
                 status |= kStatNewton;
             // density-peak fix (riemannsolver.F90:279-285)
-            if (peak_possible) {
+            if (AXIS == 2 && (a.flags & kFlagZHalo) && peak_possible) {
+                // the transposed gather of the z peak test reaches across
+                // slabs; a slab reports it instead of applying it
+                status |= kStatUnsupported;
+            } else if (peak_possible) {
                 double pk;
                 if (AXIS == 0) {
                     pk = peak_value(S.st[1][L::idx(f - 3, wtp)], S.st[1][L::idx(f - 2, wtp)],

@@ -26,6 +26,13 @@ static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int f
     for (int q = 0; q < 4; ++q) a.snap[q] = b.snap[q];
     a.peak = b.peak;
     a.g = b.g[axis];
+    // halo planes in the sweep's field order (z sweep: p, rho, vz, vy, vx)
+    static const int kPerm[3][5] = {{0, 1, 2, 3, 4}, {0, 1, 3, 2, 4}, {0, 1, 4, 3, 2}};
+    const long long plane = (long long)b.nx * b.ny;
+    for (int q = 0; q < 5; ++q) {
+        a.zlo[q] = b.zlo ? b.zlo + (long long)kPerm[axis][q] * 4 * plane : nullptr;
+        a.zhi[q] = b.zhi ? b.zhi + (long long)kPerm[axis][q] * 3 * plane : nullptr;
+    }
     a.ctl = b.ctl;
     a.k = b.k;
     a.nx = b.nx; a.ny = b.ny; a.nz = b.nz;

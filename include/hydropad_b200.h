@@ -47,7 +47,8 @@ enum {
     HP_ERR_NEGATIVE_STATE = -6,/* rho <= 0 or p <= 0 in the updated state */
     HP_ERR_NOT_ATTACHED = -7,  /* sweep requested before hp_attach_state */
     HP_ERR_STATE_MISMATCH = -8,/* host arrays differ from the attached ones */
-    HP_ERR_NO_DEVICE = -9      /* no CUDA device / wrong architecture */
+    HP_ERR_NO_DEVICE = -9,     /* no CUDA device / wrong architecture */
+    HP_ERR_UNSUPPORTED = -10   /* a case this build does not take (the density-peak fix across z slabs) */
 };
 
 enum { HP_PREC_FP64 = 0, HP_PREC_MIXED = 1 };
@@ -250,6 +251,51 @@ int hp_batch_autotune(hp_batch *b, int reps);
 /* CUDA stream of the batch (cudaStream_t) and its kernel launch count. */
 void *hp_batch_stream(hp_batch *b);
 long long hp_batch_launch_count(hp_batch *b);
+
+/* ---------------------------------------------------------------------
+ * One box split into z slabs, one per GPU (the reference's Cartesian
+ * decomposition along z, init_sys.F90:53-60, with one block per rank).
+ * Each slab is a context created by hp_init with ngridz = its own planes;
+ * the x and y sweeps are local, the z sweep reads 4 planes below and 3
+ * above from halo buffers that the caller refills before every z sweep
+ * (the ghost exchange of exchange_mesh.F90 / exchange_var.F90 between
+ * ranks), and the CFL velmax of a step is the maximum over the slabs
+ * (the MPI_Allreduce of speed.F90).  No counterpart for the step pieces in
+ * the reference, whose evolve_sys does all of it in one routine.
+ * --------------------------------------------------------------------- */
+
+/* Make ctx the slab of planes [z0, z0 + ngridz) of a periodic box of
+ * nz_global planes (ngridz >= 4): dx becomes 1/max(ngridx, ngridy,
+ * nz_global), halo buffers are allocated.  Call after hp_init, before the
+ * first step.  hp_evolve / hp_ppm_lxlylz then return HP_ERR_ARG (a slab
+ * steps through hp_step_*). */
+int hp_slab_init(hp_ctx *ctx, int nz_global, int z0);
+
+/* The planes its neighbours need, into caller DEVICE buffers in the halo
+ * layout [p, rho, vx, vy, vz][planes][ngridx*ngridy]: top4 = the top 4
+ * planes (the lower halo of the slab above), bottom3 = the bottom 3 planes
+ * (the upper halo of the slab below).  Returns when the copies are done. */
+int hp_slab_get_edges(hp_ctx *ctx, double *top4, double *bottom3);
+
+/* Refill the halos from caller DEVICE buffers of the same layout: lower4 =
+ * the 4 planes below the slab (the top4 of the slab below), upper3 = the 3
+ * planes above (the bottom3 of the slab above).  The caller's writes to
+ * them must be complete; the copies run on the context's stream. */
+int hp_slab_set_halos(hp_ctx *ctx, const double *lower4, const double *upper3);
+
+/* A step in pieces (any context, slab or not): hp_step_axis gives the axis
+ * (0 x, 1 y, 2 z) of sweep slot s of the current step (the nrot order,
+ * evolve_sys.F90:30-31); hp_step_sweep runs that sweep (a slab's z sweep
+ * reads its halos; refill them first); hp_step_velmax returns the step's
+ * velmax after slot 2; hp_step_finish runs timedet with the given velmax
+ * (the maximum over all slabs) and advances the step, returning the status
+ * accumulated since the last read.  Sweeps of a slab report
+ * HP_ERR_UNSUPPORTED if the density-peak fix could act in the z sweep (its
+ * transposed gather reaches across slabs; inert at the namelist dmax). */
+int hp_step_axis(hp_ctx *ctx, int s);
+int hp_step_sweep(hp_ctx *ctx, int s);
+int hp_step_velmax(hp_ctx *ctx, double *velmax);
+int hp_step_finish(hp_ctx *ctx, double velmax);
 
 /* Block until the context's stream is idle and return the device status
  * word accumulated since the last call (then cleared). */
