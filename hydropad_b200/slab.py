@@ -118,6 +118,16 @@ class _Slabs:
         for h in self.ctxs:
             h.timedet(v)
 
+    def autotune(self, reps: int = 1):
+        """Tile shapes from the first slab of this process (hp_autotune on a
+        scratch copy of its state), applied to every slab it holds.  The z
+        sweep's halos do not change the per-cell work, so a slab tunes like
+        a box of its own size."""
+        tiles = self.ctxs[0].autotune(reps=reps)
+        for h in self.ctxs[1:]:
+            h.set_tiles(*tiles)
+        return tiles
+
     def close(self):
         for h in self.ctxs:
             h.close()
@@ -241,6 +251,7 @@ def main(argv=None):
     sl.attach_device(*ic)
     del ic
     torch.cuda.empty_cache()
+    tiles = sl.autotune(reps=1)
     sl.start_with_cfl()
     sl.step(args.warmup)
     torch.cuda.synchronize()
@@ -260,7 +271,8 @@ def main(argv=None):
     if sl.rank == 0:
         print(json.dumps({"workload": f"{n}^3 EdS box in {world} z slab(s)", "precision": args.precision,
                           "n_gpus": world, "steps": args.steps, "ms_per_step": ms / args.steps,
-                          "cell_updates_per_s": n ** 3 * args.steps / (ms * 1e-3), "scaling": "strong"}))
+                          "cell_updates_per_s": n ** 3 * args.steps / (ms * 1e-3), "scaling": "strong",
+                          "tiles": list(tiles)}))
     sl.close()
     if world > 1:
         dist.destroy_process_group()

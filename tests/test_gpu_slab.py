@@ -77,3 +77,28 @@ def test_slab_context_refuses_whole_box_stepping():
             sl.ctxs[0].evolve(1)
     finally:
         sl.close()
+
+
+def test_dist_slab_single_rank_matches_whole_box():
+    """The per-rank form with one rank (no process group): its exchange is
+    the periodic self-copy."""
+    from hydropad_b200.api import Hydro
+    from hydropad_b200.slab import DistSlab
+    n = 20
+    prm = params_for((n, n, n), cosmo=True)
+    state = grf_state(n, seed=4)
+    with Hydro(prm, precision="mixed") as h:
+        h.attach_state(*state)
+        h.start_with_cfl()
+        h.evolve(6, graph=False)
+        whole = h.download(nbound=0)
+    sl = DistSlab(prm, precision="mixed")
+    try:
+        sl.attach_device(*_device(state))
+        sl.start_with_cfl()
+        sl.step(6)
+        split = sl.ctxs[0].download(nbound=0)
+    finally:
+        sl.close()
+    for a, b in zip(split, whole):
+        assert np.array_equal(a, b)
