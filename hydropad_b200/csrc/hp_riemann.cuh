@@ -105,15 +105,9 @@ struct PowRootBase {
 };
 
 // FP64 path: roots to a few ulp, IEEE division, the literal loop body.
-struct PowRoot : PowRootBase<2> {
-    static constexpr bool kShortNewton = false;  // the reference's Newton start value
-    __device__ __forceinline__ static double div(double a, double b) { return a / b; }
-    __device__ __forceinline__ static double div_loop(double a, double b) { return a / b; }
-};
-
-// Mixed path: the shortened Newton loop body, and divisions from the
-// hardware reciprocal estimate refined by two Newton steps plus one
-// residual correction (within an ulp or two of the IEEE quotient).
+// Divisions from the hardware reciprocal estimate refined by two Newton
+// steps plus one residual correction (within an ulp or two of the IEEE
+// quotient).
 __device__ __forceinline__ double rcp_refined(double b) {
     double r;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
@@ -122,17 +116,28 @@ __device__ __forceinline__ double rcp_refined(double b) {
     e = fma(-b, r, 1.0);
     return fma(r, e, r);
 }
+__device__ __forceinline__ double div_refined(double a, double b) {
+    const double r = rcp_refined(b);
+    const double q = a * r;
+    return fma(r, fma(-b, q, a), q);
+}
+
+// FP64 path: the reference's start value; IEEE divisions outside the
+// Newton loop, refined reciprocals (an ulp or two) for the two divisions
+// inside it -- the iterates then agree with the literal loop to a few ulp.
+struct PowRoot : PowRootBase<2> {
+    static constexpr bool kShortNewton = false;  // the reference's Newton start value
+    __device__ __forceinline__ static double div(double a, double b) { return a / b; }
+    __device__ __forceinline__ static double div_loop(double a, double b) { return div_refined(a, b); }
+};
+
 // The powers of the mixed path take one Newton step from the FP32 root
 // estimate (relative error ~1e-13, far inside the 1e-3 step tolerance of
 // the Newton iteration that uses them), and the divisions inside the loop
 // one step from the hardware reciprocal (div_loop, ~1e-13).
 struct PowRootShort : PowRootBase<1> {
     static constexpr bool kShortNewton = true;
-    __device__ __forceinline__ static double div(double a, double b) {
-        const double r = rcp_refined(b);
-        const double q = a * r;
-        return fma(r, fma(-b, q, a), q);
-    }
+    __device__ __forceinline__ static double div(double a, double b) { return div_refined(a, b); }
     __device__ __forceinline__ static double div_loop(double a, double b) {
         double r;
         asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
