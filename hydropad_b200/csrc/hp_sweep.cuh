@@ -121,12 +121,19 @@ struct SweepSmem {
     // Riemann state of face f: each slot is read and then written by the one
     // thread that solves that face
     double rs[5][P * RING];
-    int work[P * T];            // Riemann problems of the iteration, sorted by pattern
-    int cnt[P * T / 32][5];     // per-warp counts of the 5 patterns
-    int nwork;
+    int work[5][P * T];         // Riemann problems of the iteration, one bucket per pattern
+    int bcnt[2][5];             // bucket fill counts (alternate iterations use alternate rows)
     double sv[5][3 * P];        // original values of cells 0..2
     unsigned long long red[128];
 };
+
+// Barrier between stages that pass data along the pencil only: a warp
+// barrier when every warp holds whole pencil windows, else the CTA's.
+template <bool kWarp>
+__device__ __forceinline__ void pencil_sync() {
+    if constexpr (kWarp) __syncwarp();
+    else __syncthreads();
+}
 
 // One CTA's worth of work: the P pencils pid0 .. pid0+P-1 of the box `a`,
 // walked from end to end.  Every thread of the CTA calls it.
@@ -177,9 +184,27 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
 
     FaceState right;        // right state of face c (cell c), from stage B
 
-    for (int b = -4; b <= N + 3; b += T) {
+    // Barriers.  Stages load, A, B and C1 exchange data only along a pencil
+    // (ring neighbours e-2 .. e+2).  Along x a warp holds whole pencil
+    // windows (T divides 32), so a warp barrier orders them; along y/z the
+    // neighbours sit in other warps and the CTA synchronises.  C2 solves
+    // any pencil's faces and D reads any thread's C2 result: CTA barriers.
+    // The barrier before the load protects the state ring slots that the
+    // load overwrites from the previous iteration's stage D, which reads the
+    // ring only in the FP64 path and with gravity (the g ring); the mixed
+    // path's D reads the cell from global memory instead, so its y/z sweeps
+    // need no barrier there (everything else the load writes is read after
+    // the next barrier only).
+    constexpr bool kWarpPencils = AXIS == 0 && T <= 32 && (32 % T) == 0;
+    constexpr bool kDReadsRing = sizeof(R) == sizeof(double) || GRAV;
+    if (tid < 10) S.bcnt[tid / 5][tid % 5] = 0;
+    __syncthreads();
+    int par = 0;  // row of bcnt of this iteration
+
+    for (int b = -4; b <= N + 3; b += T, par ^= 1) {
         const int e = b + tl;
-        __syncthreads();
+        if constexpr (kWarpPencils) __syncwarp();
+        else if constexpr (kDReadsRing) __syncthreads();
         // ---------------- load cell e ----------------
         if (active && e >= -4 && e <= N + 2) {
             double v[5];
@@ -228,7 +253,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 S.sg[ix] = -a.g[base + stride * s];
             }
         }
-        __syncthreads();
+        pencil_sync<kWarpPencils>();
         // ---------------- A: cell c = e-1 ----------------
         {
             const int c = e - 1;
@@ -246,7 +271,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 if constexpr (GRAV) S.slg[i0] = ajside<R>(R(S.sg[im]), R(S.sg[i0]), R(S.sg[ip]));
             }
         }
-        __syncthreads();
+        pencil_sync<kWarpPencils>();
         // ---------------- B: cell c = e-3 ----------------
         {
             const int c = e - 3;
@@ -372,7 +397,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 }
             }
         }
-        __syncthreads();
+        pencil_sync<kWarpPencils>();
         // ---------------- C: face f = e-3 ----------------
         // The Riemann problems of the iteration are classified by wave
         // pattern and re-dealt to the threads sorted by pattern, so that a
@@ -395,45 +420,37 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                                                                      CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl,
                                                                      cr, k);
             }
-            const int lane = tid & 31, warp = tid >> 5;
-            const unsigned lt = (1u << lane) - 1u;
-            int rank = 0;
-#pragma unroll
-            for (int c4 = 1; c4 <= 5; ++c4) {
-                const unsigned m = __ballot_sync(0xffffffffu, mycase == c4);
-                if (lane == 0) S.cnt[warp][c4 - 1] = __popc(m);
-                if (mycase == c4) rank = __popc(m & lt);
-            }
-            __syncthreads();
-            {
-                // offset of (pattern, warp) in the sorted list: every warp
-                // scans the per-warp counts itself (lane w holds warp w's
-                // count), pattern after pattern
-                constexpr int kW = L::kThreads / 32;
-                static_assert(kW <= 32, "one lane per warp");
-                int base_off = 0, my_off = 0;
-#pragma unroll
-                for (int c4 = 0; c4 < 5; ++c4) {
-                    const int v = lane < kW ? S.cnt[lane][c4] : 0;
-                    int incl = v;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int u = __shfl_up_sync(0xffffffffu, incl, o);
-                        if (lane >= o) incl += u;
-                    }
-                    const int excl_w = __shfl_sync(0xffffffffu, incl - v, warp);  // warps before mine
-                    if (c4 + 1 == mycase) my_off = base_off + excl_w;
-                    base_off += __shfl_sync(0xffffffffu, incl, 31);           // all warps
-                }
-                if (mycase) S.work[my_off + rank] = (mycase << 24) | (tp << 16) | f;  // (pattern, pencil, face)
-                if (tid == 0) S.nwork = base_off;
-            }
+            // bucket of the pattern: the lanes of one pattern take a run of
+            // slots with one shared-memory atomic (the order of the runs
+            // within a bucket varies; every face's result does not)
+            const int lane = tid & 31;
+            const unsigned peers = __match_any_sync(0xffffffffu, mycase);
+            const int leader = __ffs(peers) - 1;
+            int off = 0;
+            if (mycase && lane == leader) off = atomicAdd(&S.bcnt[par][mycase - 1], __popc(peers));
+            off = __shfl_sync(0xffffffffu, off, leader);
+            if (mycase) S.work[mycase - 1][off + __popc(peers & ((1u << lane) - 1u))] = (tp << 16) | f;
         }
         __syncthreads();
-        // C2: solve problem number tid of the sorted list.
-        if (tid < S.nwork) {
-            const int item = S.work[tid];
-            const int pattern = item >> 24, wtp = (item >> 16) & 0xff, f = item & 0xffff;
+        // C2: solve problem number tid of the buckets laid end to end.
+        int pattern = 0, item = 0;
+        {
+            int idx = tid;
+#pragma unroll
+            for (int c4 = 0; c4 < 5; ++c4) {
+                const int n = S.bcnt[par][c4];
+                if (pattern == 0) {
+                    if (idx < n) pattern = c4 + 1;
+                    else idx -= n;
+                }
+            }
+            if (pattern) item = S.work[pattern - 1][idx];
+            // the other row was last read in the previous iteration's C2
+            // and is next filled after this iteration's last barrier
+            if (tid < 5) S.bcnt[par ^ 1][tid] = 0;
+        }
+        if (pattern) {
+            const int wtp = item >> 16, f = item & 0xffff;
             const int il = L::idx(f - 1, wtp), io = L::idx(f, wtp);
             FaceState left, rgt, out;
             left.p = double(S.ls[0][il]);
