@@ -29,10 +29,10 @@ int launch_timedet(const Box& b, int advance, cudaStream_t st);
 
 // Number of tile shapes per axis, and the pencils per CTA (P) of each
 // (the tile table in hp_sweep_launch.cuh).
-constexpr int kNumTiles = 10;
-constexpr int kTilePencils[3][kNumTiles] = {{8, 4, 8, 4, 16, 12, 8, 4, 8, 4},
-                                            {32, 16, 32, 16, 64, 32, 32, 16, 32, 16},
-                                            {32, 16, 32, 16, 64, 32, 32, 16, 32, 16}};
+constexpr int kNumTiles = 11;
+constexpr int kTilePencils[3][kNumTiles] = {{8, 4, 8, 4, 16, 12, 8, 4, 8, 4, 16},
+                                            {32, 16, 32, 16, 64, 32, 32, 16, 32, 16, 16},
+                                            {32, 16, 32, 16, 64, 32, 32, 16, 32, 16, 16}};
 
 struct BatchLaunch;  // hp_sweep.cuh
 

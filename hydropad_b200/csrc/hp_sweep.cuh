@@ -121,9 +121,10 @@ struct SweepSmem {
     // Riemann state of face f: each slot is read and then written by the one
     // thread that solves that face
     double rs[5][P * RING];
-    int work[5][P * T];         // Riemann problems of the iteration, one bucket per pattern
+    unsigned short work[5][P * T];  // Riemann problems of the iteration (by the thread index
+                                    // that classified them), one bucket per pattern
     int bcnt[2][5];             // bucket fill counts (alternate iterations use alternate rows)
-    double sv[5][3 * P];        // original values of cells 0..2
+    R sv[5][3 * P];             // original values of cells 0..2 (they only refill the state ring)
     unsigned long long red[128];
 };
 
@@ -145,6 +146,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     using CT = typename Policy::CT;
     using L = SweepLayout<AXIS, P, T, RING>;
     static_assert((RING & (RING - 1)) == 0 && RING >= T + 6, "ring too small");
+    static_assert(P * T <= 65536, "work items are 16-bit thread indices");
 
     const int tid = threadIdx.x;
     const int tl = AXIS == 0 ? (tid % T) : (tid / P);
@@ -230,7 +232,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 for (int q = 0; q < 5; ++q) v[q] = a.f[q][g];
                 if (e >= 0 && e < 3) {
 #pragma unroll
-                    for (int q = 0; q < 5; ++q) S.sv[q][e * P + tp] = v[q];
+                    for (int q = 0; q < 5; ++q) S.sv[q][e * P + tp] = R(v[q]);
                 }
                 if ((a.flags & kFlagSnapshot) && e >= 0 && e < N) {
                     // natural order p, vx, vy, vz
@@ -429,7 +431,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             int off = 0;
             if (mycase && lane == leader) off = atomicAdd(&S.bcnt[par][mycase - 1], __popc(peers));
             off = __shfl_sync(0xffffffffu, off, leader);
-            if (mycase) S.work[mycase - 1][off + __popc(peers & ((1u << lane) - 1u))] = (tp << 16) | f;
+            if (mycase) S.work[mycase - 1][off + __popc(peers & ((1u << lane) - 1u))] = (unsigned short)tid;
         }
         __syncthreads();
         // C2: solve problem number tid of the buckets laid end to end.
@@ -450,7 +452,9 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             if (tid < 5) S.bcnt[par ^ 1][tid] = 0;
         }
         if (pattern) {
-            const int wtp = item >> 16, f = item & 0xffff;
+            // the classifying thread's pencil and face
+            const int wtp = AXIS == 0 ? (item / T) : (item % P);
+            const int f = b - 3 + (AXIS == 0 ? (item % T) : (item / P));
             const int il = L::idx(f - 1, wtp), io = L::idx(f, wtp);
             FaceState left, rgt, out;
             left.p = double(S.ls[0][il]);
