@@ -311,20 +311,33 @@ __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, dou
     return riemann_newton_short<Pow>(pstar, vstar, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
 }
 
-// Pattern 1: two shocks, riemannsolver.F90:73-109.  The Newton iteration
-// for p*, u* runs in FP64; S is the type of the sampling that follows it
-// (which wave lands on the face, and the density behind it): double in the
-// FP64 path, float in the mixed path, as its closed two-rarefaction form.
-template <class Pow, class S = double>
-__device__ __forceinline__ bool riemann_two_shocks(const FaceState& L, const FaceState& R, double& pm, double& vxm,
-                                                   double& rhom, const Consts& k) {
-    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
-    pm = fmax2(pleft, pright);
+// Patterns 1 and 2 share the Newton iteration for p*, u* (riemann.F90,
+// FP64 in both paths); each has its own start value and its own sampling
+// of the solution at the face.  The caller runs one Newton loop for the
+// faces of both patterns, so a warp that holds faces of both runs the loop
+// once.  S is the type of the sampling (which wave lands on the face, and
+// the density behind it): double in the FP64 path, float in the mixed path,
+// as its closed two-rarefaction form.
+
+// Start value of pattern 1, two shocks (riemannsolver.F90:77): the larger
+// pressure; the mixed path replaces it by the two-rarefaction estimate.
+// The FP64 path's riemann_newton then applies the reference's own start
+// value when that is positive.
+template <class Pow>
+__device__ __forceinline__ double start_two_shocks(const FaceState& L, const FaceState& R, const Consts& k) {
+    double pm = fmax2(L.p, R.p);
     if constexpr (Pow::kShortNewton) {
-        const double st = mixed_newton_start(pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+        const double st = mixed_newton_start(L.p, R.p, L.rho, R.rho, L.u, R.u, k);
         if (st > 0.0) pm = st;
     }
-    const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
+    return pm;
+}
+
+// Sampling of pattern 1 after the Newton solve, riemannsolver.F90:82-109.
+template <class S>
+__device__ __forceinline__ void sample_two_shocks(const FaceState& L, const FaceState& R, double& pm, double& vxm,
+                                                  double& rhom, const Consts& k) {
+    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
     const S pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
     const S rl = S(rholeft), rr = S(rhoright);
     const S rhoshock1 = rhoshock<S>(pmS, S(pleft), rl, g1);
@@ -338,30 +351,31 @@ __device__ __forceinline__ bool riemann_two_shocks(const FaceState& L, const Fac
     else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = double(rhoshock2);
     else if (vshock1 <= S(0) && vxm > 0.0) rhom = double(rhoshock1);
     else { pm = pleft; vxm = vxleft; rhom = rholeft; }
-    return ok;
 }
 
-// Pattern 2: one shock and one rarefaction, riemannsolver.F90:113-184.
-// Newton in FP64, sampling in S with the powers of PowS (as pattern 1).
-template <class Pow, class S = double, class PowS = Pow>
-__device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, const FaceState& R, double cleft,
-                                                          double cright, double& pm, double& vxm, double& rhom,
-                                                          const Consts& k) {
+// Start value of pattern 2, one shock and one rarefaction
+// (riemannsolver.F90:117-119): the reference's two-rarefaction guess, which
+// the mixed path forms in FP64 only when its own FP32 estimate fails.
+template <class Pow>
+__device__ __forceinline__ double start_shock_rarefaction(const FaceState& L, const FaceState& R, double cleft,
+                                                          double cright, const Consts& k) {
+    if constexpr (Pow::kShortNewton) {
+        const double pm = mixed_newton_start(L.p, R.p, L.rho, R.rho, L.u, R.u, k);
+        if (pm > 0.0) return pm;
+    }
+    return Pow::prm((cleft + cright + (L.u - R.u) * (k.gamma - 1.0) * 0.5) /
+                        (cleft / Pow::pm(L.p, k) + cright / Pow::pm(R.p, k)),
+                    k);
+}
+
+// Sampling of pattern 2 after the Newton solve, riemannsolver.F90:124-184,
+// with the powers of PowS.
+template <class S, class PowS>
+__device__ __forceinline__ void sample_shock_rarefaction(const FaceState& L, const FaceState& R, double cleft,
+                                                         double cright, double& pm, double& vxm, double& rhom,
+                                                         const Consts& k) {
     const double gamma = k.gamma;
     const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
-    // the start value of riemann.F90 (which its guess replaces when that is
-    // positive); the mixed path forms it in FP64 only when its own FP32
-    // start value fails
-    bool need_start = true;
-    if constexpr (Pow::kShortNewton) {
-        pm = mixed_newton_start(pleft, pright, rholeft, rhoright, vxleft, vxright, k);
-        need_start = !(pm > 0.0);
-    }
-    if (need_start)
-        pm = Pow::prm((cleft + cright + (vxleft - vxright) * (gamma - 1.0) * 0.5) /
-                          (cleft / Pow::pm(pleft, k) + cright / Pow::pm(pright, k)),
-                      k);
-    const bool ok = riemann_newton<Pow>(pm, vxm, pleft, pright, rholeft, rhoright, vxleft, vxright, k);
     const S gS = S(gamma), pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
     if (pleft >= pright) {
         const S rr = S(rhoright), rl = S(rholeft);
@@ -400,7 +414,6 @@ __device__ __forceinline__ bool riemann_shock_rarefaction(const FaceState& L, co
             vxm = double(rarwave<S>(S(vxright), vxmS, vtail2, vhead2));
         }
     }
-    return ok;
 }
 
 // Pattern 3: two rarefactions, riemannsolver.F90:188-227 (closed form).
@@ -498,8 +511,18 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
                                                    FaceState& out, const Consts& k, const StepScalars& s) {
     double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
     bool ok = true;
-    if (pattern == 1) {
-        ok = riemann_two_shocks<Pow, RareT>(L, R, pm, vxm, rhom, k);
+    if (pattern == 1 || pattern == 2) {
+        double cleft = 0.0, cright = 0.0;
+        if (pattern == 2) {
+            cleft = sqrt(k.gamma * L.p / L.rho);
+            cright = sqrt(k.gamma * R.p / R.rho);
+            pm = start_shock_rarefaction<Pow>(L, R, cleft, cright, k);
+        } else {
+            pm = start_two_shocks<Pow>(L, R, k);
+        }
+        ok = riemann_newton<Pow>(pm, vxm, L.p, R.p, L.rho, R.rho, L.u, R.u, k);
+        if (pattern == 1) sample_two_shocks<RareT>(L, R, pm, vxm, rhom, k);
+        else sample_shock_rarefaction<RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
     } else if (pattern == 3) {
         const RareT g = RareT(k.gamma);
         const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);
@@ -525,10 +548,9 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
                 else riemann_two_rarefactions<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cl, cr, pm, vxm, rhom, k);
             }
         }
-    } else if (pattern == 2 || pattern == 4) {
+    } else if (pattern == 4) {
         const double cleft = sqrt(k.gamma * L.p / L.rho), cright = sqrt(k.gamma * R.p / R.rho);
-        if (pattern == 2) ok = riemann_shock_rarefaction<Pow, RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
-        else riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
+        riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
     }
     riemann_finish(L, R, pm, vxm, rhom, out, s);
     return ok;
