@@ -106,6 +106,19 @@ struct SweepLayout {
     }
 };
 
+// Buckets of the Riemann problems, in the order the solving threads take
+// them: shock + rarefaction with the rarefaction on the left (pL >= pR),
+// two shocks, shock + rarefaction with the rarefaction on the right, then
+// the closed forms.  The three Newton buckets share the iteration, and
+// neighbouring buckets differ in the wave on one side only, so a warp that
+// straddles two of them diverges on one side of the loop body.
+constexpr int kBuckets = 6;
+// 1 + bucket of a face of pattern 1..5 (pattern 2: rare_left = pL >= pR)
+__device__ __forceinline__ int bucket_of(int pattern, bool rare_left) {
+    return pattern == 2 ? (rare_left ? 1 : 3) : (pattern == 1 ? 2 : pattern + 1);
+}
+__device__ __forceinline__ int pattern_of_bucket(int c) { return (c == 0 || c == 2) ? 2 : (c == 1 ? 1 : c); }
+
 template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
 struct SweepSmem {
     using R = typename Policy::R;
@@ -121,9 +134,9 @@ struct SweepSmem {
     // Riemann state of face f: each slot is read and then written by the one
     // thread that solves that face
     double rs[5][P * RING];
-    unsigned short work[5][P * T];  // Riemann problems of the iteration (by the thread index
-                                    // that classified them), one bucket per pattern
-    int bcnt[2][5];             // bucket fill counts (alternate iterations use alternate rows)
+    unsigned short work[kBuckets][P * T];  // Riemann problems of the iteration (by the thread
+                                           // index that classified them), in buckets
+    int bcnt[2][kBuckets];      // bucket fill counts (alternate iterations use alternate rows)
     R sv[5][3 * P];             // original values of cells 0..2 (they only refill the state ring)
     unsigned long long red[128];
 };
@@ -199,7 +212,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     // the next barrier only).
     constexpr bool kWarpPencils = AXIS == 0 && T <= 32 && (32 % T) == 0;
     constexpr bool kDReadsRing = sizeof(R) == sizeof(double) || GRAV;
-    if (tid < 10) S.bcnt[tid / 5][tid % 5] = 0;
+    if (tid < 2 * kBuckets) S.bcnt[tid / kBuckets][tid % kBuckets] = 0;
     __syncthreads();
     int par = 0;  // row of bcnt of this iteration
 
@@ -408,7 +421,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         // them).  C1 classifies and publishes the right states.
         {
             const int f = e - 3;
-            int mycase = 0;
+            int bucket = 0;  // 1 + bucket of the face, 0: no face
             if (active && f >= 0 && f <= N) {
                 const int io = L::idx(f, tp);
                 S.rs[0][io] = right.p;
@@ -418,20 +431,21 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 S.rs[4][io] = right.w;
                 const int il = L::idx(f - 1, tp);
                 CT cl, cr;
-                mycase = riemann_classify<CT, typename Policy::PowC>(CT(S.ls[0][il]), CT(right.p), CT(S.ls[1][il]),
-                                                                     CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl,
-                                                                     cr, k);
+                const CT pl = CT(S.ls[0][il]), pr = CT(right.p);
+                const int pattern = riemann_classify<CT, typename Policy::PowC>(
+                    pl, pr, CT(S.ls[1][il]), CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl, cr, k);
+                bucket = bucket_of(pattern, pl >= pr);
             }
-            // bucket of the pattern: the lanes of one pattern take a run of
-            // slots with one shared-memory atomic (the order of the runs
-            // within a bucket varies; every face's result does not)
+            // the lanes of one bucket take a run of its slots with one
+            // shared-memory atomic (the order of the runs within a bucket
+            // varies; every face's result does not)
             const int lane = tid & 31;
-            const unsigned peers = __match_any_sync(0xffffffffu, mycase);
+            const unsigned peers = __match_any_sync(0xffffffffu, bucket);
             const int leader = __ffs(peers) - 1;
             int off = 0;
-            if (mycase && lane == leader) off = atomicAdd(&S.bcnt[par][mycase - 1], __popc(peers));
+            if (bucket && lane == leader) off = atomicAdd(&S.bcnt[par][bucket - 1], __popc(peers));
             off = __shfl_sync(0xffffffffu, off, leader);
-            if (mycase) S.work[mycase - 1][off + __popc(peers & ((1u << lane) - 1u))] = (unsigned short)tid;
+            if (bucket) S.work[bucket - 1][off + __popc(peers & ((1u << lane) - 1u))] = (unsigned short)tid;
         }
         __syncthreads();
         // C2: solve problem number tid of the buckets laid end to end.
@@ -439,17 +453,20 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         {
             int idx = tid;
 #pragma unroll
-            for (int c4 = 0; c4 < 5; ++c4) {
-                const int n = S.bcnt[par][c4];
+            for (int c = 0; c < kBuckets; ++c) {
+                const int n = S.bcnt[par][c];
                 if (pattern == 0) {
-                    if (idx < n) pattern = c4 + 1;
-                    else idx -= n;
+                    if (idx < n) {
+                        pattern = pattern_of_bucket(c);
+                        item = S.work[c][idx];
+                    } else {
+                        idx -= n;
+                    }
                 }
             }
-            if (pattern) item = S.work[pattern - 1][idx];
             // the other row was last read in the previous iteration's C2
             // and is next filled after this iteration's last barrier
-            if (tid < 5) S.bcnt[par ^ 1][tid] = 0;
+            if (tid < kBuckets) S.bcnt[par ^ 1][tid] = 0;
         }
         if (pattern) {
             // the classifying thread's pencil and face
