@@ -160,8 +160,13 @@ class Scheduler:
     engine interface: ``now()`` (seconds since the trace start),
     ``wait_until(t)``, ``create(req) -> box`` (allocate + initial
     conditions), ``add(box)``, ``step(k)`` (asynchronous), ``sync()``,
-    ``finish(box) -> result`` (download and remove from the batch),
-    ``release(box)``."""
+    ``detach(box)`` (leave the batch), ``finish(box) -> result``
+    (download), ``release(box)``.
+
+    When members finish, the scheduler waits for the batch, detaches them,
+    enqueues the next chunk of the remaining members and only then reads
+    the finished boxes back, so that the downloads overlap the GPU's work
+    on the others."""
 
     def __init__(self, engine, budget_bytes: int, capacity: int = 64, chunk: int = 8, keep_results: bool = False):
         self.engine = engine
@@ -178,6 +183,7 @@ class Scheduler:
         active: list = []
         resident = 0
         stall_since = None
+        inflight = False  # a chunk of the current members is enqueued and not yet accounted
         for r in pending:
             if box_bytes(r.side) > self.budget:
                 raise ValueError(f"request {r.rid} (side {r.side}) can never fit the HBM budget")
@@ -212,16 +218,21 @@ class Scheduler:
                 if pending:
                     eng.wait_until(pending[0].arrival)
                 continue
-            k = min(self.chunk, min(m.remaining for m in active))
-            eng.step(k)
-            st.steps_launched += k
-            for m in active:
-                m.remaining -= k
+            if not inflight:
+                self._launch(eng, st, active)
+            inflight = False
             done = [m for m in active if m.remaining == 0]
             if done:
                 tc = time.perf_counter()
                 eng.sync()
                 st.sync_s += time.perf_counter() - tc
+                for m in done:
+                    eng.detach(m.box)
+                    active.remove(m)
+                if active:
+                    # the others run on while the finished boxes are read back
+                    self._launch(eng, st, active)
+                    inflight = True
                 for m in done:
                     tc = time.perf_counter()
                     res = eng.finish(m.box)
@@ -231,11 +242,19 @@ class Scheduler:
                                                   res if self.keep_results else None))
                     eng.release(m.box)
                     resident -= box_bytes(m.req.side)
-                    active.remove(m)
         if stall_since is not None:
             st.stall_seconds += eng.now() - stall_since
         st.wall = eng.now()
         return st
+
+    def _launch(self, eng, st: ServeStats, active: list):
+        """Enqueue a chunk of steps of every member, never past the step
+        count of the member that finishes first."""
+        k = min(self.chunk, min(m.remaining for m in active))
+        eng.step(k)
+        st.steps_launched += k
+        for m in active:
+            m.remaining -= k
 
 
 class GpuEngine:
@@ -256,6 +275,7 @@ class GpuEngine:
         self.pool: dict = {}
         self.pool_bytes = int(pool_bytes)
         self.pooled = 0
+        self.reused = 0      # requests served by a kept context
         self.initial = {}
         self.t0 = time.perf_counter()
 
@@ -283,6 +303,7 @@ class GpuEngine:
         if free:
             h = free.pop()
             self.pooled -= box_bytes(req.side)
+            self.reused += 1
             h.set_scalars(self.initial[req.side])
         else:
             h = Hydro(self.params(req.side), precision=self.precision, device=self.device)
@@ -304,8 +325,10 @@ class GpuEngine:
     def sync(self):
         self.batch.synchronize()
 
-    def finish(self, h):
+    def detach(self, h):
         self.batch.remove(h)
+
+    def finish(self, h):
         return h.download(nbound=0) if self.download else None
 
     def release(self, h):
@@ -341,6 +364,18 @@ def tune_tiles(precision: str, sides=(64, 128, 192, 256), device: int = 0):
     return tuple(tiles)
 
 
+def warm_up(sides=range(32, 257, 16), device: int = 0):
+    """Server start-up: one initial-condition draw per admissible side, so
+    that the FFT plans and kernels of the generator exist before the first
+    request (the first draw of a side in a process costs tens of ms)."""
+    import torch
+
+    from . import ics
+    for side in sides:
+        ics.grf_eds_device(int(side), seed=0, device=f"cuda:{device}", noise="device")
+    torch.cuda.synchronize(device)
+
+
 def run_alone(req: Request, precision: str, tiles=None, device: int = 0):
     """One request advanced by itself through hp_evolve (the parity
     reference of the serving path); returns the final state."""
@@ -358,10 +393,13 @@ def run_alone(req: Request, precision: str, tiles=None, device: int = 0):
 
 
 def run_serving(requests: int = 100, rate: float = 200.0, trace_seed: int = 2024, precision: str = "mixed",
-                budget_bytes: int = 0, capacity: int = 64, chunk: int = 8, tiles=None, pool_bytes: int = 0,
+                budget_bytes: int = 0, capacity: int = 64, chunk: int = 8, tiles=None, pool_bytes: int = -1,
                 world: int = 1, rank: int = 0, device: int = 0):
     """This rank's share of the serving trace (:func:`shard_trace`), then one
-    host gather: returns (merged statistics of every rank, tiles)."""
+    host gather: returns (merged statistics of every rank, tiles).
+    ``pool_bytes`` < 0 keeps finished contexts for reuse up to a tenth of the
+    budget (a context that is kept is not freed, and freeing device memory
+    waits for the whole device)."""
     import torch
 
     from .shard import gather_objects, shard_trace
@@ -370,8 +408,11 @@ def run_serving(requests: int = 100, rate: float = 200.0, trace_seed: int = 2024
     if budget_bytes <= 0:
         free, _total = torch.cuda.mem_get_info(device)
         budget_bytes = int(0.8 * free)
+    if pool_bytes < 0:
+        pool_bytes = budget_bytes // 10
     if tiles is None:
         tiles = tune_tiles(precision, device=device)
+    warm_up(device=device)
     eng = GpuEngine(precision, capacity=capacity, tiles=tiles, device=device, pool_bytes=pool_bytes)
     try:
         sched = Scheduler(eng, budget_bytes - eng.pool_bytes, capacity=capacity, chunk=chunk)
@@ -397,7 +438,8 @@ def main(argv=None):
     ap.add_argument("--chunk", type=int, default=8)
     ap.add_argument("--tiles", default="auto",
                     help="batched-sweep tile per axis 'x,y,z', or 'auto' (tuned on a warm-up batch)")
-    ap.add_argument("--pool-gb", type=float, default=0.0, help="keep finished contexts for reuse up to this size")
+    ap.add_argument("--pool-gb", type=float, default=-1.0,
+                    help="keep finished contexts for reuse up to this size (default: a tenth of the budget)")
     args = ap.parse_args(argv)
 
     import os
@@ -413,8 +455,9 @@ def main(argv=None):
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=3600))
     torch.cuda.set_device(dev)
     tiles = None if args.tiles == "auto" else tuple(int(t) for t in args.tiles.split(","))
+    pool = int(args.pool_gb * 1e9) if args.pool_gb >= 0 else -1
     st, tiles = run_serving(args.requests, args.rate, args.trace_seed, args.precision, int(args.budget_gb * 1e9),
-                            args.capacity, args.chunk, tiles, int(args.pool_gb * 1e9), world, rank, dev)
+                            args.capacity, args.chunk, tiles, pool, world, rank, dev)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -2,11 +2,14 @@
 
 
 class ModelEngine:
-    """Simulated clock: a batch step costs (cells of the members) / rate
-    seconds; creating a box costs ``create_s``."""
+    """Simulated clock.  Host work (creating a box) advances the clock; a
+    batch step is enqueued like a GPU launch: it costs (cells of the
+    members) / rate seconds of device time, starting when the device is free,
+    and the host sees its end only at ``sync``."""
 
     def __init__(self, rate=1e9, create_s=1e-3):
         self.t = 0.0
+        self.busy = 0.0           # device time at which the enqueued work ends
         self.rate = rate
         self.create_s = create_s
         self.members = []
@@ -28,15 +31,20 @@ class ModelEngine:
         self.members.append(box)
 
     def step(self, k):
-        self.t += k * sum(b["req"].cells for b in self.members) / self.rate
+        start = max(self.t, self.busy)
+        self.busy = start + k * sum(b["req"].cells for b in self.members) / self.rate
         for b in self.members:
             b["steps"] += k
+        self.log.append(("step", k, len(self.members)))
 
     def sync(self):
-        pass
+        self.t = max(self.t, self.busy)
+
+    def detach(self, box):
+        self.members.remove(box)
 
     def finish(self, box):
-        self.members.remove(box)
+        self.log.append(("finish", box["req"].rid, self.t))
         return box["steps"]
 
     def release(self, box):

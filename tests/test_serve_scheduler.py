@@ -75,6 +75,20 @@ def test_capacity_limits_members():
     assert max(seen) == 3
 
 
+def test_results_read_back_while_the_others_run():
+    # request 0 ends with the first chunk: the scheduler detaches it and
+    # enqueues request 1's next chunk before reading request 0 back
+    tr = [Request(0, 0.0, 32, 8, 0), Request(1, 0.0, 32, 24, 1)]
+    eng = ModelEngine()
+    st = Scheduler(eng, budget_bytes=box_bytes(32) * 2, capacity=4, chunk=8).run(tr)
+    ev = [e for e in eng.log if e[0] in ("step", "finish")]
+    assert ev[0] == ("step", 8, 2) and ev[1] == ("step", 8, 1)
+    assert ev[2][:2] == ("finish", 0)
+    assert st.steps_launched == 24
+    done = {c.rid: c.done for c in st.completed}
+    assert done[0] < done[1]
+
+
 def test_rejects_request_larger_than_budget():
     with pytest.raises(ValueError):
         Scheduler(ModelEngine(), budget_bytes=box_bytes(64), capacity=4).run([Request(0, 0.0, 128, 10, 0)])
