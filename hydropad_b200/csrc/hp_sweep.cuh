@@ -34,7 +34,9 @@
 //
 // Thread layout.  Along x (AXIS 0) a warp holds 32 consecutive cells of one
 // pencil; along y/z a warp holds 32 neighbouring pencils (consecutive x) at
-// the same sweep position.  Both give 256-byte coalesced rows.
+// the same sweep position for the load and the update (256-byte coalesced
+// rows) and 32/T neighbouring pencils x the T cells of the window for the
+// stages in between (SweepLayout).
 #pragma once
 #include "hp_device.cuh"
 #include "hp_physics.cuh"
@@ -96,13 +98,30 @@ __device__ __forceinline__ long long axis_stride(int nx, int ny) {
     return AXIS == 0 ? 1 : (AXIS == 1 ? (long long)nx : (long long)nx * ny);
 }
 
+// Ring layout and the thread layout of stages A, B and C1.  Along x a warp
+// holds whole pencil windows in both layouts.  Along y/z the load and the
+// update keep 32 neighbouring pencils per warp (256-byte rows); when T
+// divides 32, stages A, B and C1 re-deal the threads so that a warp holds
+// kPw = 32/T neighbouring pencils x the T cells of the window, and those
+// stages pass data within the warp.  The y/z ring rows are padded by kPw
+// pencils, which keeps both layouts free of shared-memory bank conflicts.
 template <int AXIS, int P, int T, int RING>
 struct SweepLayout {
+    static constexpr bool kYZWarp = AXIS != 0 && (32 % T) == 0 && (P % (32 / T)) == 0;
+    static constexpr int kPw = kYZWarp ? 32 / T : 1;
+    static constexpr int kStride = AXIS == 0 ? RING : (kYZWarp ? P + kPw : P);
     static constexpr int kThreads = P * T;
-    static constexpr int kCells = P * RING;
+    static constexpr int kCells = AXIS == 0 ? P * RING : kStride * RING;
     __device__ __forceinline__ static int idx(int cell, int tp) {
         const int slot = cell & (RING - 1);
-        return AXIS == 0 ? tp * RING + slot : slot * P + tp;
+        return AXIS == 0 ? tp * RING + slot : slot * kStride + tp;
+    }
+    // cell offset in the window and pencil of thread t in stages A, B, C1
+    __device__ __forceinline__ static int wcell(int t) {
+        return AXIS == 0 ? t % T : (kYZWarp ? (t & 31) / kPw : t / P);
+    }
+    __device__ __forceinline__ static int wpencil(int t) {
+        return AXIS == 0 ? t / T : (kYZWarp ? (t >> 5) * kPw + (t & 31) % kPw : t % P);
     }
 };
 
@@ -122,18 +141,19 @@ __device__ __forceinline__ int pattern_of_bucket(int c) { return (c == 0 || c ==
 template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
 struct SweepSmem {
     using R = typename Policy::R;
-    static constexpr int kG = GRAV ? P * RING : 1;
-    R st[5][P * RING];          // state ring: p, rho, u, v, w (FP32 copy in the mixed path)
+    static constexpr int kC = SweepLayout<AXIS, P, T, RING>::kCells;
+    static constexpr int kG = GRAV ? kC : 1;
+    R st[5][kC];                // state ring: p, rho, u, v, w (FP32 copy in the mixed path)
     double sg[kG];              // gravity ring: g = -gforce of this sweep's axis
     R slg[kG];                  // ajside slope of g
-    R sl[5][P * RING];          // ajside slopes
-    R d2[P * RING];             // dda second difference of rho
-    unsigned char pf[P * RING]; // flattening flag of pair (c, c+1)
-    R ls[5][P * RING];          // traced left state (face c+1) from cell c
+    R sl[5][kC];                // ajside slopes
+    R d2[kC];                   // dda second difference of rho
+    unsigned char pf[kC];       // flattening flag of pair (c, c+1)
+    R ls[5][kC];                // traced left state (face c+1) from cell c
     // traced right state of face f (from cell f), replaced in place by the
     // Riemann state of face f: each slot is read and then written by the one
     // thread that solves that face
-    double rs[5][P * RING];
+    double rs[5][kC];
     unsigned short work[kBuckets][P * T];  // Riemann problems of the iteration (by the thread
                                            // index that classified them), in buckets
     int bcnt[2][kBuckets];      // bucket fill counts (alternate iterations use alternate rows)
@@ -166,6 +186,9 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     const int tp = AXIS == 0 ? (tid / T) : (tid % P);
     const long long pid = pid0 + tp;
     const bool active = pid < a.npencil;
+    // the same in the layout of stages A, B and C1
+    const int tlw = L::wcell(tid), tpw = L::wpencil(tid);
+    const bool activew = pid0 + tpw < a.npencil;
     const int N = a.nsweep;
     const long long base = pencil_base<AXIS>(active ? pid : 0, a.nx, a.ny);
     const long long stride = axis_stride<AXIS>(a.nx, a.ny);
@@ -201,9 +224,10 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
 
     // Barriers.  Stages load, A, B and C1 exchange data only along a pencil
     // (ring neighbours e-2 .. e+2).  Along x a warp holds whole pencil
-    // windows (T divides 32), so a warp barrier orders them; along y/z the
-    // neighbours sit in other warps and the CTA synchronises.  C2 solves
-    // any pencil's faces and D reads any thread's C2 result: CTA barriers.
+    // windows (T divides 32), so warp barriers order them; along y/z the
+    // threads change layout after the load (a CTA barrier) and then hold
+    // whole pencil windows for A, B and C1 (warp barriers).  C2 solves any
+    // pencil's faces and D reads any thread's C2 result: CTA barriers.
     // The barrier before the load protects the state ring slots that the
     // load overwrites from the previous iteration's stage D, which reads the
     // ring only in the FP64 path and with gravity (the g ring); the mixed
@@ -211,13 +235,15 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     // need no barrier there (everything else the load writes is read after
     // the next barrier only).
     constexpr bool kWarpPencils = AXIS == 0 && T <= 32 && (32 % T) == 0;
+    constexpr bool kWarpStages = kWarpPencils || L::kYZWarp;  // A -> B -> C1 within a warp
     constexpr bool kDReadsRing = sizeof(R) == sizeof(double) || GRAV;
     if (tid < 2 * kBuckets) S.bcnt[tid / kBuckets][tid % kBuckets] = 0;
     __syncthreads();
     int par = 0;  // row of bcnt of this iteration
 
     for (int b = -4; b <= N + 3; b += T, par ^= 1) {
-        const int e = b + tl;
+        const int e = b + tl;    // load and update layout
+        const int ew = b + tlw;  // layout of stages A, B and C1
         if constexpr (kWarpPencils) __syncwarp();
         else if constexpr (kDReadsRing) __syncthreads();
         // ---------------- load cell e ----------------
@@ -268,12 +294,12 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 S.sg[ix] = -a.g[base + stride * s];
             }
         }
-        pencil_sync<kWarpPencils>();
+        pencil_sync<kWarpPencils>();  // y/z: the threads change layout here
         // ---------------- A: cell c = e-1 ----------------
         {
-            const int c = e - 1;
-            if (active && c >= -3 && c <= N + 1) {
-                const int im = L::idx(c - 1, tp), i0 = L::idx(c, tp), ip = L::idx(c + 1, tp);
+            const int c = ew - 1;
+            if (activew && c >= -3 && c <= N + 1) {
+                const int im = L::idx(c - 1, tpw), i0 = L::idx(c, tpw), ip = L::idx(c + 1, tpw);
                 bool flag = false;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
@@ -286,14 +312,14 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 if constexpr (GRAV) S.slg[i0] = ajside<R>(R(S.sg[im]), R(S.sg[i0]), R(S.sg[ip]));
             }
         }
-        pencil_sync<kWarpPencils>();
+        pencil_sync<kWarpStages>();
         // ---------------- B: cell c = e-3 ----------------
         {
-            const int c = e - 3;
-            if (active && c >= -1 && c <= N) {
+            const int c = ew - 3;
+            if (activew && c >= -1 && c <= N) {
                 int ic[5];
 #pragma unroll
-                for (int o = 0; o < 5; ++o) ic[o] = L::idx(c - 2 + o, tp);
+                for (int o = 0; o < 5; ++o) ic[o] = L::idx(c - 2 + o, tpw);
                 const bool fl_any = S.pf[ic[0]] | S.pf[ic[1]] | S.pf[ic[2]] | S.pf[ic[3]];
                 const R flat = fl_any ? flatv_ : R(0);
                 const R pm1 = R(S.st[0][ic[1]]), p0 = R(S.st[0][ic[2]]), pp1 = R(S.st[0][ic[3]]);
@@ -412,7 +438,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 }
             }
         }
-        pencil_sync<kWarpPencils>();
+        pencil_sync<kWarpStages>();
         // ---------------- C: face f = e-3 ----------------
         // The Riemann problems of the iteration are classified by wave
         // pattern and re-dealt to the threads sorted by pattern, so that a
@@ -420,16 +446,16 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         // different code paths; faces of a smooth flow alternate between
         // them).  C1 classifies and publishes the right states.
         {
-            const int f = e - 3;
+            const int f = ew - 3;
             int bucket = 0;  // 1 + bucket of the face, 0: no face
-            if (active && f >= 0 && f <= N) {
-                const int io = L::idx(f, tp);
+            if (activew && f >= 0 && f <= N) {
+                const int io = L::idx(f, tpw);
                 S.rs[0][io] = right.p;
                 S.rs[1][io] = right.rho;
                 S.rs[2][io] = right.u;
                 S.rs[3][io] = right.v;
                 S.rs[4][io] = right.w;
-                const int il = L::idx(f - 1, tp);
+                const int il = L::idx(f - 1, tpw);
                 CT cl, cr;
                 const CT pl = CT(S.ls[0][il]), pr = CT(right.p);
                 const int pattern = riemann_classify<CT, typename Policy::PowC>(
@@ -470,8 +496,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         }
         if (pattern) {
             // the classifying thread's pencil and face
-            const int wtp = AXIS == 0 ? (item / T) : (item % P);
-            const int f = b - 3 + (AXIS == 0 ? (item % T) : (item / P));
+            const int wtp = L::wpencil(item);
+            const int f = b - 3 + L::wcell(item);
             const int il = L::idx(f - 1, wtp), io = L::idx(f, wtp);
             FaceState left, rgt, out;
             left.p = double(S.ls[0][il]);
