@@ -105,16 +105,20 @@ __device__ __forceinline__ long long axis_stride(int nx, int ny) {
 // kPw = 32/T neighbouring pencils x the T cells of the window, and those
 // stages pass data within the warp.  The y/z ring rows are padded by kPw
 // pencils, which keeps both layouts free of shared-memory bank conflicts.
+// Along x a warp holds 32/T pencils when T < 32; the slots of its k-th
+// pencil are XOR-ed with k*T (RING a multiple of 32), for the same reason.
 template <int AXIS, int P, int T, int RING>
 struct SweepLayout {
     static constexpr bool kYZWarp = AXIS != 0 && (32 % T) == 0 && (P % (32 / T)) == 0;
     static constexpr int kPw = kYZWarp ? 32 / T : 1;
     static constexpr int kStride = AXIS == 0 ? RING : (kYZWarp ? P + kPw : P);
     static constexpr int kThreads = P * T;
-    static constexpr int kCells = AXIS == 0 ? P * RING : kStride * RING;
+    static constexpr int kCells = kStride * (AXIS == 0 ? P : RING);
+    static_assert(AXIS != 0 || T >= 32 || ((32 % T) == 0 && RING % 32 == 0), "x swizzle");
     __device__ __forceinline__ static int idx(int cell, int tp) {
         const int slot = cell & (RING - 1);
-        return AXIS == 0 ? tp * RING + slot : slot * kStride + tp;
+        if (AXIS == 0) return tp * RING + (T < 32 ? slot ^ ((tp & (32 / T - 1)) * T) : slot);
+        return slot * kStride + tp;
     }
     // cell offset in the window and pencil of thread t in stages A, B, C1
     __device__ __forceinline__ static int wcell(int t) {
