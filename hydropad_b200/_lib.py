@@ -18,6 +18,8 @@ HP_ERR = {
 }
 HP_PREC_FP64 = 0
 HP_PREC_MIXED = 1
+HP_VARIANT_STENCIL = 0   # the STENCIL build's sweeps (default)
+HP_VARIANT_PENCIL = 1    # the non-STENCIL build's full-pencil ppm() (hydro/ppm.F90)
 
 
 class HpParams(C.Structure):
@@ -58,6 +60,7 @@ EXPORTS = (
     "hp_batch_create", "hp_batch_destroy", "hp_batch_add", "hp_batch_remove", "hp_batch_size",
     "hp_batch_step", "hp_batch_synchronize", "hp_batch_member", "hp_batch_set_tiles", "hp_batch_get_tiles",
     "hp_batch_autotune", "hp_batch_stream", "hp_batch_launch_count",
+    "hp_set_variant", "hp_get_variant", "hp_attach_cho", "hp_ppmsolver_pencil",
 )
 _NOT_INT = ("hp_stream", "hp_strerror", "hp_launch_count", "hp_batch_member", "hp_batch_stream",
             "hp_batch_launch_count")
@@ -96,6 +99,10 @@ def lib():
     L.hp_download_state.argtypes = [cp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int]
     L.hp_ppmsolver.argtypes = [cp, dp, dp, dp, dp, dp, dp, dp, dp, ip, ip, ip, ip, ip]
     L.hp_ppm_lxlylz.argtypes = [cp, C.c_int]
+    L.hp_set_variant.argtypes = [cp, C.c_int]
+    L.hp_get_variant.argtypes = [cp]
+    L.hp_attach_cho.argtypes = [cp, dp, C.c_int, C.c_int, C.c_int, C.c_int]
+    L.hp_ppmsolver_pencil.argtypes = [cp] + [dp] * 14 + [ip] * 5
     L.hp_speed.argtypes = [cp, dp]
     L.hp_timedet.argtypes = [cp, C.c_double]
     L.hp_evolve.argtypes = [cp, C.c_int, C.c_int]

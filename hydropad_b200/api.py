@@ -163,6 +163,44 @@ class Hydro:
                                   C.byref(nx), C.byref(ny), C.byref(nz), C.byref(nb), C.byref(nd))
         L.check(rc, "hp_ppmsolver")
 
+    def set_variant(self, variant: str):
+        """``"stencil"`` (default) or ``"pencil"``: the sweep of
+        :meth:`ppm_lxlylz`, :meth:`evolve` and the step pieces -- the STENCIL
+        build's sweeps or the non-STENCIL build's full-pencil ppm()
+        (hydro/ppm.F90; FP64 only)."""
+        code = {"stencil": L.HP_VARIANT_STENCIL, "pencil": L.HP_VARIANT_PENCIL}[variant]
+        L.check(L.lib().hp_set_variant(self._ctx, code), "hp_set_variant")
+
+    def get_variant(self) -> str:
+        return "pencil" if L.lib().hp_get_variant(self._ctx) == L.HP_VARIANT_PENCIL else "stencil"
+
+    def attach_cho(self, cho3d):
+        """The cho3d array the full-pencil solver reads at density peaks
+        (ghosted Fortran order, the shape of the attached arrays), or None."""
+        if cho3d is None:
+            L.check(L.lib().hp_attach_cho(self._ctx, None, 0, 0, 0, 0), "hp_attach_cho")
+            self._cho = None
+            return
+        c = np.asfortranarray(cho3d, dtype=np.float64)
+        nx, ny, nz = c.shape
+        nb = (nx - self.params.shape[0]) // 2
+        L.check(L.lib().hp_attach_cho(self._ctx, _dptr(c), nx, ny, nz, nb), "hp_attach_cho")
+        self._cho = c
+
+    def ppmsolver_pencil(self, ndirection: int):
+        """One full-pencil sweep through the drop-in of the non-STENCIL
+        ppmsolver (its argument list; the *3dnew arrays are not written)."""
+        a = self._host
+        nx, ny, nz = (C.c_int(v) for v in a[0].shape)
+        nb = C.c_int(self.params.nbound)
+        nd = C.c_int(int(ndirection))
+        g = getattr(self, "_gforce", None)
+        cho = getattr(self, "_cho", None)
+        rc = L.lib().hp_ppmsolver_pencil(self._ctx, *[_dptr(x) for x in a], None if cho is None else _dptr(cho),
+                                         None, None if g is None else _dptr(g), *[None] * 6,
+                                         C.byref(nx), C.byref(ny), C.byref(nz), C.byref(nb), C.byref(nd))
+        L.check(rc, "hp_ppmsolver_pencil")
+
     def ppm_lxlylz(self, nrot: int):
         L.check(L.lib().hp_ppm_lxlylz(self._ctx, int(nrot)), "hp_ppm_lxlylz")
         L.check(L.lib().hp_synchronize(self._ctx), "hp_ppm_lxlylz")

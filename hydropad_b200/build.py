@@ -35,6 +35,8 @@ SOURCES = [
     # sweeps with the static gravity source, same flags as above
     ("hp_kernels_grav_fp64.cu", ["--fmad=false"]),
     ("hp_kernels_grav_mixed.cu", MIXED),
+    # the non-STENCIL build's full-pencil solver (FP64), same flags
+    ("hp_kernels_pencil_fp64.cu", ["--fmad=false"]),
     # persistent batched sweeps (many boxes per launch), same flags as above
     ("hp_batch_fp64.cu", ["--fmad=false"]),
     ("hp_batch_mixed.cu", MIXED),

@@ -157,7 +157,7 @@ int do_sweep(hp_ctx* x, int axis, int flags) {
     int n = 0;
     if (x->slab && axis == 2) {
         flags |= hp::kFlagZHalo;  // no pre-pass: its transposed gather would cross slabs
-    } else {
+    } else if (!x->box.pencil) {  // the full-pencil solver's peak test reads its own window
         n = hp::launch_peak_prepass(x->box, axis, bslot, x->stream);
         if (n < 0) return HP_ERR_CUDA;
     }
@@ -357,6 +357,7 @@ int hp_finalize(hp_ctx* x) {
     cudaFree(x->box.zlo);
     cudaFree(x->box.zhi);
     for (int q = 0; q < 3; ++q) cudaFree(x->box.g[q]);
+    cudaFree(x->cho_dev);
     cudaFree(x->box.ctl);
     if (x->ctl_pinned) cudaFreeHost(x->ctl_pinned);
     if (x->stream) cudaStreamDestroy(x->stream);
@@ -743,6 +744,7 @@ int hp_autotune(hp_ctx* x, int reps) {
 
 int hp_slab_init(hp_ctx* x, int nz_global, int z0) {
     if (!x || x->slab) return HP_ERR_ARG;
+    if (x->box.pencil) return HP_ERR_UNSUPPORTED;
     const int nz = x->box.nz;
     if (nz < 4 || z0 < 0 || nz_global < nz || z0 + nz > nz_global) return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(x->dev));
@@ -842,5 +844,71 @@ int hp_device_fields(hp_ctx* x, double** p, double** rho, double** vx, double** 
 }
 
 long long hp_launch_count(hp_ctx* x) { return x ? x->launches : 0; }
+
+int hp_set_variant(hp_ctx* x, int variant) {
+    if (!x || (variant != HP_VARIANT_STENCIL && variant != HP_VARIANT_PENCIL)) return HP_ERR_ARG;
+    if (variant == HP_VARIANT_PENCIL && (x->prm.precision != HP_PREC_FP64 || x->slab)) return HP_ERR_UNSUPPORTED;
+    HP_CUDA(cudaSetDevice(x->dev));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    drop_graphs(x);
+    x->box.pencil = variant == HP_VARIANT_PENCIL ? 1 : 0;
+    return HP_OK;
+}
+
+int hp_get_variant(hp_ctx* x) {
+    if (!x) return HP_ERR_ARG;
+    return x->box.pencil ? HP_VARIANT_PENCIL : HP_VARIANT_STENCIL;
+}
+
+int hp_attach_cho(hp_ctx* x, const double* cho3d, int nx, int ny, int nz, int nbound) {
+    if (!x) return HP_ERR_ARG;
+    HP_CUDA(cudaSetDevice(x->dev));
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    drop_graphs(x);
+    if (!cho3d) {
+        cudaFree(x->cho_dev);
+        x->cho_dev = nullptr;
+        x->box.cho = nullptr;
+        x->host_cho = nullptr;
+        return HP_OK;
+    }
+    if (nbound < 0 || nx != x->box.nx + 2 * nbound || ny != x->box.ny + 2 * nbound || nz != x->box.nz + 2 * nbound)
+        return HP_ERR_ARG;
+    if (!x->cho_dev) {
+        const size_t n = (size_t)x->box.nx * x->box.ny * x->box.nz;
+        int rc = cuda_fail(cudaMalloc(&x->cho_dev, n * sizeof(double)));
+        if (rc != HP_OK) return rc;
+    }
+    int rc = upload_field(x, cho3d, x->cho_dev, nbound);
+    if (rc != HP_OK) return rc;
+    HP_CUDA(cudaStreamSynchronize(x->stream));
+    x->box.cho = x->cho_dev;
+    x->host_cho = cho3d;
+    return HP_OK;
+}
+
+int hp_ppmsolver_pencil(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, double* vy3d, double* vz3d,
+                        double* cho3d, double* nes3d, const double* gforce, double* p3dnew, double* rho3dnew,
+                        double* vx3dnew, double* vy3dnew, double* vz3dnew, double* cho3dnew, const int* nx,
+                        const int* ny, const int* nz, const int* nbound, const int* ndirection) {
+    (void)nes3d;
+    (void)p3dnew; (void)rho3dnew; (void)vx3dnew; (void)vy3dnew; (void)vz3dnew; (void)cho3dnew;
+    if (!x || !nx || !ny || !nz || !nbound || !ndirection) return HP_ERR_ARG;
+    if (x->prm.precision != HP_PREC_FP64 || x->slab) return HP_ERR_UNSUPPORTED;
+    if (!x->attached) return HP_ERR_NOT_ATTACHED;
+    if (gforce != x->host_g || cho3d != x->host_cho) return HP_ERR_STATE_MISMATCH;
+    if (*ndirection < 1 || *ndirection > 3) return HP_ERR_ARG;
+    if (*nx != x->hnx || *ny != x->hny || *nz != x->hnz || *nbound != x->hnb) return HP_ERR_STATE_MISMATCH;
+    const double* given[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
+    for (int q = 0; q < 5; ++q)
+        if (given[q] != x->host[q]) return HP_ERR_STATE_MISMATCH;
+    HP_CUDA(cudaSetDevice(x->dev));
+    const int was = x->box.pencil;
+    x->box.pencil = 1;
+    int rc = do_sweep(x, *ndirection - 1, 0);
+    x->box.pencil = was;
+    if (rc != HP_OK) return rc;
+    return hp_synchronize(x);
+}
 
 }  // extern "C"

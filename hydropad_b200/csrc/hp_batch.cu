@@ -289,6 +289,7 @@ int hp_batch_add(hp_batch* b, hp_ctx* x) {
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     if (x->box.g[0]) return HP_ERR_ARG;  // the batched sweeps carry no gravity source
     if (x->slab) return HP_ERR_ARG;      // nor the halos of a z slab
+    if (x->box.pencil) return HP_ERR_ARG;  // nor the full-pencil solver
     if (std::find(b->members.begin(), b->members.end(), x) != b->members.end()) return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(b->dev));
     HP_CUDA(cudaStreamSynchronize(x->stream));  // the member's own work is finished

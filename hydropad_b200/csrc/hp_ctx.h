@@ -26,6 +26,8 @@ struct hp_ctx {
     size_t stage_bytes;
     int slab;                 // 1: a z slab of a larger periodic box (hp_slab_init)
     int nz_global, z0;
+    double* cho_dev;          // attached cho3d (dense) for the full-pencil solver, or null
+    const double* host_cho;   // the attached host cho3d array, or null
 };
 
 namespace hp {

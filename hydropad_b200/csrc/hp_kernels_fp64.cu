@@ -15,8 +15,11 @@
 namespace hp {
 
 int launch_sweep_grav_fp64(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st);
+int launch_sweep_pencil_fp64(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st);
 
 int launch_sweep_fp64(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
+    // the full-pencil solver ignores gforce (ppm.F90:93,102)
+    if (b.pencil) return launch_sweep_pencil_fp64(b, axis, tile, bslot, flags, st);
     if (b.g[0]) return launch_sweep_grav_fp64(b, axis, tile, bslot, flags, st);
     return launch_sweep_policy<PolicyFP64>(b, axis, tile, bslot, flags, st);
 }

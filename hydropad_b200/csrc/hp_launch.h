@@ -15,9 +15,11 @@ struct Box {
     double* g[3];      // gforce components x, y, z (dense, natural layout), or null: gravity off
     double* zlo;       // slab of a z-split box: 4 halo planes below, [p,rho,vx,vy,vz][4][nx*ny], or null
     double* zhi;       // 3 halo planes above, [5][3][nx*ny], or null
+    const double* cho; // cho3d marker of each cell for the full-pencil solver (dense), or null: zeros
     DevCtl* ctl;       // device control block
     Consts k;
     int nx, ny, nz;
+    int pencil;        // 1: the non-STENCIL build's full-pencil solver (hydro/ppm.F90); FP64 only
 };
 
 // Launches return the number of kernels launched (>= 0) or -1 on a launch error.

@@ -266,4 +266,72 @@ __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& 
     w = vznew;
 }
 
+// New total energy of a cell from its two faces, ppm.F90:563-567 with the
+// gravity term zero (ghalf = 0, :93): the update's and the neighbours' value.
+__device__ __forceinline__ double etot_new(const FaceState& f1, const FaceState& f2, double etot, const Consts& k,
+                                           const StepScalars& s) {
+    const double gamma = k.gamma, rgamma1 = k.rgamma1;
+    const double flux1 = (gamma * f1.p * rgamma1 + 0.5 * f1.rho * (f1.u * f1.u + f1.v * f1.v + f1.w * f1.w)) * f1.u;
+    const double flux2 = (gamma * f2.p * rgamma1 + 0.5 * f2.rho * (f2.u * f2.u + f2.v * f2.v + f2.w * f2.w)) * f2.u;
+    return etot + s.rdtath * (flux1 - flux2) * k.rdx;
+}
+
+// The update of the non-STENCIL build's full-pencil solver, ppm.F90:544-606
+// (the gravity terms vanish: ghalf = 0, :93) and its dual-energy switch
+// and fallbacks, :611-658: the switch divides by the largest new total
+// energy of the cell (eeleft, its own, eeright: the neighbours' values, 0
+// beyond the pencil's updated cells).  At a density peak (the cell's old
+// rho above dmax x each old neighbour's), cho = 1 raises pmean to the
+// peak pressure and cho = 2 takes it from the internal energy (:585-594).
+template <class Div = DivIEEE>
+__device__ __forceinline__ void integrate_pencil(const FaceState& f1, const FaceState& f2, double& pres, double& rho,
+                                                 double& u, double& v, double& w, double etot, double eint,
+                                                 const Consts& k, const StepScalars& s, double eeleft, double eeright,
+                                                 bool peak, double cho) {
+    const double gamma = k.gamma, rgamma1 = k.rgamma1, rdtath = s.rdtath, rdx = k.rdx;
+    double flux1 = f1.rho * f1.u;
+    double flux2 = f2.rho * f2.u;
+    double rhonew = rho + rdtath * (flux1 - flux2) * rdx;
+    flux1 = f1.rho * f1.u * f1.u + f1.p;
+    flux2 = f2.rho * f2.u * f2.u + f2.p;
+    const double vxnew = Div::div(u * rho + rdtath * (flux1 - flux2) * rdx, rhonew);
+    flux1 = f1.v * f1.u * f1.rho;
+    flux2 = f2.v * f2.u * f2.rho;
+    const double vynew = Div::div(rho * v + rdtath * (flux1 - flux2) * rdx, rhonew);
+    flux1 = f1.w * f1.u * f1.rho;
+    flux2 = f2.w * f2.u * f2.rho;
+    const double vznew = Div::div(rho * w + rdtath * (flux1 - flux2) * rdx, rhonew);
+    const double etotnew = etot_new(f1, f2, etot, k, s);
+    double pmean = (f1.p + f2.p) * 0.5;
+    if (peak) {
+        if (cho == 1.0) {
+            const double maxp = (f1.u - f2.u) * rho * fmax2(0.0, f1.u - f2.u);
+            pmean = fmax2(pmean, maxp);
+        } else if (cho == 2.0) {
+            pmean = (gamma - 1.0) * eint;
+        }
+    }
+    double eintnew = eint + rdtath * pmean * (f1.u - f2.u) * rdx;
+    flux1 = (f1.p * f1.u) * rgamma1;
+    flux2 = (f2.p * f2.u) * rgamma1;
+    eintnew = eintnew + rdtath * (flux1 - flux2) * rdx;
+    if (eintnew < 0.0) eintnew = eint;
+    const double ee2 = fmax2(fmax2(eeleft, etotnew), eeright);
+    const double vvv = vxnew * vxnew + vynew * vynew + vznew * vznew;
+    const double eeaux = etotnew - 0.5 * rhonew * vvv;
+    const double ee1 = Div::div(eeaux, ee2);
+    if (ee1 >= k.eta2) eintnew = eeaux;
+    const double ee0 = Div::div(eeaux, etotnew);
+    double pnew;
+    if (ee0 >= k.eta1) pnew = (gamma - 1.0) * eeaux;
+    else pnew = (gamma - 1.0) * eintnew;
+    if (eintnew <= 0.0) pnew = pres;
+    if (rhonew <= 0.0) rhonew = rho;
+    pres = pnew;
+    rho = rhonew;
+    u = vxnew;
+    v = vynew;
+    w = vznew;
+}
+
 }  // namespace hp

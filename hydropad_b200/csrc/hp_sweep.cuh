@@ -53,6 +53,9 @@ struct SweepArgs {
     // above the slab, [field][plane][nx*ny] in the sweep's field order
     const double* zlo[5];
     const double* zhi[5];
+    // full-pencil sweeps: the cho3d marker of each cell (natural layout), or
+    // null for zeros
+    const double* cho;
     DevCtl* ctl;
     Consts k;
     int nx, ny, nz;
@@ -142,11 +145,13 @@ __device__ __forceinline__ int bucket_of(int pattern, bool rare_left) {
 }
 __device__ __forceinline__ int pattern_of_bucket(int c) { return (c == 0 || c == 2) ? 2 : (c == 1 ? 1 : c); }
 
-template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
+template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false, bool PENCIL = false>
 struct SweepSmem {
     using R = typename Policy::R;
     static constexpr int kC = SweepLayout<AXIS, P, T, RING>::kCells;
     static constexpr int kG = GRAV ? kC : 1;
+    static constexpr int kE = PENCIL ? kC : 1;
+    double se[kE];              // full-pencil sweeps: new total energy of each cell
     R st[5][kC];                // state ring: p, rho, u, v, w (FP32 copy in the mixed path)
     double sg[kG];              // gravity ring: g = -gforce of this sweep's axis
     R slg[kG];                  // ajside slope of g
@@ -175,15 +180,21 @@ __device__ __forceinline__ void pencil_sync() {
 
 // One CTA's worth of work: the P pencils pid0 .. pid0+P-1 of the box `a`,
 // walked from end to end.  Every thread of the CTA calls it.
-template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false>
+// PENCIL: the non-STENCIL build's full-pencil solver (hydro/ppm.F90)
+// instead of the STENCIL sweep; see the notes at its four differences.
+template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false, bool PENCIL = false>
 __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0,
-                                              SweepSmem<AXIS, P, T, RING, Policy, GRAV>& S) {
+                                              SweepSmem<AXIS, P, T, RING, Policy, GRAV, PENCIL>& S) {
     using R = typename Policy::R;
     using Pow = typename Policy::Pow;
     using CT = typename Policy::CT;
     using L = SweepLayout<AXIS, P, T, RING>;
     static_assert((RING & (RING - 1)) == 0 && RING >= T + 6, "ring too small");
     static_assert(P * T <= 65536, "work items are 16-bit thread indices");
+    static_assert(!(GRAV && PENCIL), "the full-pencil solver has no gravity source (ppm.F90:93,102)");
+    // the full-pencil solver's update runs one cell later than the STENCIL
+    // one (its dual-energy switch reads the new total energy of the next cell)
+    constexpr int kLag = PENCIL ? 1 : 0;
 
     const int tid = threadIdx.x;
     const int tl = AXIS == 0 ? (tid % T) : (tid / P);
@@ -245,7 +256,73 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     __syncthreads();
     int par = 0;  // row of bcnt of this iteration
 
-    for (int b = -4; b <= N + 3; b += T, par ^= 1) {
+    using DivD = typename Policy::DivD;
+    // D's inputs: the Riemann states of faces d and d+1 of this thread's
+    // pencil, and the cell's FP64 state: from the ring in the FP64 path; the
+    // mixed path keeps an FP32 ring and reads it again from global memory,
+    // which still holds it (only this thread writes cell d)
+    auto load_faces = [&](int d, FaceState& f1, FaceState& f2) {
+        const int id = L::idx(d, tp), id1 = L::idx(d + 1, tp);
+        f1.p = S.rs[0][id];
+        f1.rho = S.rs[1][id];
+        f1.u = S.rs[2][id];
+        f1.v = S.rs[3][id];
+        f1.w = S.rs[4][id];
+        f2.p = S.rs[0][id1];
+        f2.rho = S.rs[1][id1];
+        f2.u = S.rs[2][id1];
+        f2.v = S.rs[3][id1];
+        f2.w = S.rs[4][id1];
+    };
+    auto cell_state = [&](int d, long long g, double& p, double& rho, double& u, double& v, double& w) {
+        if constexpr (sizeof(R) == sizeof(double)) {
+            const int id = L::idx(d, tp);
+            p = S.st[0][id]; rho = S.st[1][id]; u = S.st[2][id]; v = S.st[3][id]; w = S.st[4][id];
+        } else {
+            p = a.f[0][g]; rho = a.f[1][g]; u = a.f[2][g]; v = a.f[3][g]; w = a.f[4][g];
+        }
+    };
+    // D's epilogue: expand, store, and the step's reductions
+    auto finish_cell = [&](long long g, double p, double rho, double u, double v, double w) {
+        if (a.flags & kFlagExpand) {
+            // expand.F90:161-176 with the step-start snapshot
+            const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
+            const double vx_o = zero_old ? 0.0 : a.snap[1][g];
+            const double vy_o = zero_old ? 0.0 : a.snap[2][g];
+            const double vz_o = zero_old ? 0.0 : a.snap[3][g];
+            const double p_o = zero_old ? 0.0 : a.snap[0][g];
+            const double un_o = AXIS == 0 ? vx_o : (AXIS == 1 ? vy_o : vz_o);
+            const double v_o = AXIS == 0 ? vy_o : (AXIS == 1 ? vx_o : vy_o);
+            const double w_o = AXIS == 0 ? vz_o : (AXIS == 1 ? vz_o : vx_o);
+            u = (2.0 * u - afact * un_o) * afact2;
+            v = (2.0 * v - afact * v_o) * afact2;
+            w = (2.0 * w - afact * w_o) * afact2;
+            const double ppp = p;
+            p = (p - afact * p_o) * afact1;
+            if (p <= 0.0) p = ppp > 0.0 ? ppp : p_o;
+        }
+        a.f[0][g] = p;
+        a.f[1][g] = rho;
+        a.f[2][g] = u;
+        a.f[3][g] = v;
+        a.f[4][g] = w;
+        const unsigned long long kr = dkey(rho);
+        kmin = kr < kmin ? kr : kmin;
+        kmax = kr > kmax ? kr : kmax;
+        if (a.flags & kFlagSpeed) {
+            // speed.F90:25-28
+            const double vs = sqrt(k.gamma * p / rho);
+            double vm = fabs(u) + vs;
+            vm = fmax2(vm, fabs(v) + vs);
+            vm = fmax2(vm, fabs(w) + vs);
+            const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
+            kvel = kb > kvel ? kb : kvel;
+        }
+        if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) status |= kStatNaN;
+        else if (rho <= 0.0 || p <= 0.0) status |= kStatNegative;
+    };
+
+    for (int b = -4; b <= N + 3 + kLag; b += T, par ^= 1) {
         const int e = b + tl;    // load and update layout
         const int ew = b + tlw;  // layout of stages A, B and C1
         if constexpr (kWarpPencils) __syncwarp();
@@ -254,10 +331,10 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         if (active && e >= -4 && e <= N + 2) {
             double v[5];
             // Cell e-N (0..2) is overwritten by stage D of the iteration that
-            // holds e' = e-N+4; until then global memory still has the
+            // holds e' = e-N+4+kLag; until then global memory still has the
             // original value (and the save area may not be written yet when
             // the pencil is shorter than one iteration).
-            const bool from_save = e >= N && (e + 4) / T > (e - N + 8) / T;
+            const bool from_save = e >= N && (e + 4) / T > (e - N + 8 + kLag) / T;
             const bool from_halo = AXIS == 2 && (a.flags & kFlagZHalo) && (e < 0 || e >= N);
             if (from_halo) {
                 // a z slab's neighbours: planes -4..-1 below, N..N+2 above
@@ -332,7 +409,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 const R addrho = R(0.5) * gam_ * fabs(rp1 - rm1) / fmin2(rm1, rp1);
                 const bool steep = addrho >= addp;
                 const R u0 = R(S.st[2][ic[2]]);
-                const R cc = sqrt(gam_ * p0 / r0);
+                // sound speed of the characteristic speeds: the cell's own
+                // (order2interp.F90:56-57); the full-pencil solver takes the
+                // next cell's (ppm.F90:106-107: cbar = c(i), c(i+1) beside
+                // vxbar(2), vxbar(3) = cells i-1, i)
+                const R cc = PENCIL ? sqrt(gam_ * pp1 / rp1) : sqrt(gam_ * p0 / r0);
                 // characteristic speeds of the cell (order2interp.F90:194-196,221-223)
                 const R lm = (u0 - cc) * rat_, l0 = u0 * rat_, lp = (u0 + cc) * rat_;
                 // x = y/dx of fl/fr (ppm_functs.F90:59-84); the right-side
@@ -524,7 +605,13 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 status |= kStatUnsupported;
             } else if (peak_possible) {
                 double pk;
-                if (AXIS == 0) {
+                if constexpr (PENCIL) {
+                    // the full-pencil solver's 5-cell window along the sweep:
+                    // rhobar(1..4) = cells f-2..f+1, vxbar(2..3) = f-1, f
+                    pk = peak_value(S.st[1][L::idx(f - 2, wtp)], S.st[1][L::idx(f - 1, wtp)],
+                                    S.st[1][L::idx(f, wtp)], S.st[1][L::idx(f + 1, wtp)],
+                                    S.st[2][L::idx(f - 1, wtp)], S.st[2][L::idx(f, wtp)], k.dmax);
+                } else if (AXIS == 0) {
                     pk = peak_value(S.st[1][L::idx(f - 3, wtp)], S.st[1][L::idx(f - 2, wtp)],
                                     S.st[1][L::idx(f - 1, wtp)], S.st[1][L::idx(f, wtp)],
                                     S.st[2][L::idx(f - 2, wtp)], S.st[2][L::idx(f - 1, wtp)], k.dmax);
@@ -546,76 +633,66 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         }
         __syncthreads();
         // ---------------- D: cell d = e-4 ----------------
-        {
+        if constexpr (PENCIL) {
+            // D1: the new total energy of cell e-4, which the dual-energy
+            // switch of its neighbours reads (ppm.F90:611-621)
+            {
+                const int d = e - 4;
+                if (active && d >= 0 && d < N) {
+                    const long long g = base + stride * d;
+                    FaceState f1, f2;
+                    load_faces(d, f1, f2);
+                    double p, rho, u, v, w;
+                    cell_state(d, g, p, rho, u, v, w);
+                    // total() of the pencil's order (normal, transverse 1,
+                    // transverse 2; ppmsolver.F90:173,301,429)
+                    S.se[L::idx(d, tp)] = etot_new(f1, f2, total_energy(p, rho, u, v, w, k.rgamma1), k, sc);
+                }
+            }
+            pencil_sync<kWarpPencils>();
+            // D2: the update of cell e-5
+            {
+                const int d = e - 5;
+                if (active && d >= 0 && d < N) {
+                    const long long g = base + stride * d;
+                    FaceState f1, f2;
+                    load_faces(d, f1, f2);
+                    double p, rho, u, v, w;
+                    cell_state(d, g, p, rho, u, v, w);
+                    const double etot = total_energy(p, rho, u, v, w, k.rgamma1);
+                    const double eint = p * k.rgamma1;
+                    // the neighbours' new total energy, 0 beyond the pencil's
+                    // updated cells (ppm.F90:613-617)
+                    const double eel = d > 0 ? S.se[L::idx(d - 1, tp)] : 0.0;
+                    const double eer = d < N - 1 ? S.se[L::idx(d + 1, tp)] : 0.0;
+                    // density peak of the cell against its old neighbours
+                    // (ppm.F90:585-586)
+                    const bool peak = rho > k.dmax * double(S.st[1][L::idx(d - 1, tp)]) &&
+                                      rho > k.dmax * double(S.st[1][L::idx(d + 1, tp)]);
+                    const double cho = (peak && a.cho) ? a.cho[g] : 0.0;
+                    integrate_pencil<DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, eel, eer, peak, cho);
+                    finish_cell(g, p, rho, u, v, w);
+                }
+            }
+        } else {
             const int d = e - 4;
             if (active && d >= 0 && d < N) {
-                const int id = L::idx(d, tp), id1 = L::idx(d + 1, tp);
-                FaceState f1, f2;
-                f1.p = S.rs[0][id];
-                f1.rho = S.rs[1][id];
-                f1.u = S.rs[2][id];
-                f1.v = S.rs[3][id];
-                f1.w = S.rs[4][id];
-                f2.p = S.rs[0][id1];
-                f2.rho = S.rs[1][id1];
-                f2.u = S.rs[2][id1];
-                f2.v = S.rs[3][id1];
-                f2.w = S.rs[4][id1];
-                // the cell's FP64 state: from the ring in the FP64 path; the
-                // mixed path keeps an FP32 ring and reads it again from
-                // global memory, which still holds it (only this thread
-                // writes cell d, below)
                 const long long g = base + stride * d;
+                FaceState f1, f2;
+                load_faces(d, f1, f2);
                 double p, rho, u, v, w;
-                if constexpr (sizeof(R) == sizeof(double)) {
-                    p = S.st[0][id]; rho = S.st[1][id]; u = S.st[2][id]; v = S.st[3][id]; w = S.st[4][id];
-                } else {
-                    p = a.f[0][g]; rho = a.f[1][g]; u = a.f[2][g]; v = a.f[3][g]; w = a.f[4][g];
-                }
+                cell_state(d, g, p, rho, u, v, w);
                 // total() with the natural component order (ppmsolver.F90:149,277,405)
                 double etot;
                 if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
                 else etot = total_energy(p, rho, u, v, w, k.rgamma1);
                 const double eint = p * k.rgamma1;
-                using DivD = typename Policy::DivD;
-                if constexpr (GRAV) integrate<true, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[id]);
-                else integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
-                if (a.flags & kFlagExpand) {
-                    // expand.F90:161-176 with the step-start snapshot
-                    const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
-                    const double vx_o = zero_old ? 0.0 : a.snap[1][g];
-                    const double vy_o = zero_old ? 0.0 : a.snap[2][g];
-                    const double vz_o = zero_old ? 0.0 : a.snap[3][g];
-                    const double p_o = zero_old ? 0.0 : a.snap[0][g];
-                    const double un_o = AXIS == 0 ? vx_o : (AXIS == 1 ? vy_o : vz_o);
-                    const double v_o = AXIS == 0 ? vy_o : (AXIS == 1 ? vx_o : vy_o);
-                    const double w_o = AXIS == 0 ? vz_o : (AXIS == 1 ? vz_o : vx_o);
-                    u = (2.0 * u - afact * un_o) * afact2;
-                    v = (2.0 * v - afact * v_o) * afact2;
-                    w = (2.0 * w - afact * w_o) * afact2;
-                    const double ppp = p;
-                    p = (p - afact * p_o) * afact1;
-                    if (p <= 0.0) p = ppp > 0.0 ? ppp : p_o;
+                if constexpr (GRAV) {
+                    integrate<true, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[L::idx(d, tp)]);
+                } else {
+                    integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
                 }
-                a.f[0][g] = p;
-                a.f[1][g] = rho;
-                a.f[2][g] = u;
-                a.f[3][g] = v;
-                a.f[4][g] = w;
-                const unsigned long long kr = dkey(rho);
-                kmin = kr < kmin ? kr : kmin;
-                kmax = kr > kmax ? kr : kmax;
-                if (a.flags & kFlagSpeed) {
-                    // speed.F90:25-28
-                    const double vs = sqrt(k.gamma * p / rho);
-                    double vm = fabs(u) + vs;
-                    vm = fmax2(vm, fabs(v) + vs);
-                    vm = fmax2(vm, fabs(w) + vs);
-                    const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
-                    kvel = kb > kvel ? kb : kvel;
-                }
-                if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) status |= kStatNaN;
-                else if (rho <= 0.0 || p <= 0.0) status |= kStatNegative;
+                finish_cell(g, p, rho, u, v, w);
             }
         }
     }
@@ -628,11 +705,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
 // MINB > 1 asks the compiler for at most 65536/(P*T*MINB) registers per
 // thread so that MINB CTAs fit on one SM (more warps to hide the latency of
 // the FP64 Riemann chains, at the price of spills).
-template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false>
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false, bool PENCIL = false>
 __global__ void __launch_bounds__(P* T, MINB) ppm_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy, GRAV>*>(smem_raw);
-    sweep_pencils<AXIS, P, T, RING, Policy, GRAV>(a, (long long)blockIdx.x * P, S);
+    auto& S = *reinterpret_cast<SweepSmem<AXIS, P, T, RING, Policy, GRAV, PENCIL>*>(smem_raw);
+    sweep_pencils<AXIS, P, T, RING, Policy, GRAV, PENCIL>(a, (long long)blockIdx.x * P, S);
 }
 
 // Many boxes per launch (the ensemble and the serving batch).  Work item i

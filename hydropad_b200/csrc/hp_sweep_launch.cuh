@@ -33,6 +33,7 @@ static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int f
         a.zlo[q] = b.zlo ? b.zlo + (long long)kPerm[axis][q] * 4 * plane : nullptr;
         a.zhi[q] = b.zhi ? b.zhi + (long long)kPerm[axis][q] * 3 * plane : nullptr;
     }
+    a.cho = b.cho;
     a.ctl = b.ctl;
     a.k = b.k;
     a.nx = b.nx; a.ny = b.ny; a.nz = b.nz;
@@ -43,11 +44,11 @@ static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int f
     return a;
 }
 
-template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false>
+template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false, bool PENCIL = false>
 static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
     const SweepArgs a = make_sweep_args(b, AXIS, bslot, flags);
-    const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy, GRAV>);
-    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB, GRAV>;
+    const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy, GRAV, PENCIL>);
+    auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB, GRAV, PENCIL>;
     static bool attr_set = false;  // per instantiation (one process drives one device)
     if (!attr_set) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -80,11 +81,13 @@ static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
 HP_TILE_TABLE(HP_TILE_CHECK)
 #undef HP_TILE_CHECK
 
-// GRAV: the instantiation with the gravity source (a box with gforce).
-template <class Policy, bool GRAV = false>
+// GRAV: the instantiation with the gravity source (a box with gforce);
+// PENCIL: the non-STENCIL build's full-pencil solver.
+template <class Policy, bool GRAV = false, bool PENCIL = false>
 static int launch_sweep_policy(const Box& b, int axis, int tile, int bslot, int flags, cudaStream_t st) {
 #define HP_TILE_CASE(AX, TI, P, T, RING, MINB) \
-    if (axis == AX && tile == TI) return launch_sweep_t<AX, P, T, RING, Policy, MINB, GRAV>(b, bslot, flags, st);
+    if (axis == AX && tile == TI)                \
+        return launch_sweep_t<AX, P, T, RING, Policy, MINB, GRAV, PENCIL>(b, bslot, flags, st);
     HP_TILE_TABLE(HP_TILE_CASE)
 #undef HP_TILE_CASE
     return -1;

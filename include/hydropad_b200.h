@@ -314,6 +314,47 @@ const char *hp_strerror(int code);
 /* Number of kernels launched by this context since creation. */
 long long hp_launch_count(hp_ctx *ctx);
 
+/* ---- The non-STENCIL build's full-pencil solver --------------------------
+ * A build of the reference without -DSTENCIL sweeps each pencil whole with
+ * SUBROUTINE ppm (hydro/ppm.F90:1-662), called by the #else branches of
+ * ppmsolver (hydro/ppmsolver.F90:162-190, 290-318, 418-446), writes the
+ * *3dnew arrays and copies them back with savetn (hydropad/savetn.F90).
+ * Its arithmetic differs from the STENCIL sweep in four places, all kept:
+ * the characteristic speeds of cell k use the sound speed of cell k+1
+ * (ppm.F90:106-107), the density-peak fix reads cells f-2..f+1 of the
+ * sweep's own pencil, pmean takes the cho3d-dependent values at density
+ * peaks (ppm.F90:585-594), and the dual-energy switch divides by the largest
+ * new total energy of the cell and its neighbours, 0 beyond the pencil's
+ * updated cells (ppm.F90:611-621); it has no gravity source (ppm.F90:93,102
+ * zero it).  FP64 only; not for z slabs or batches. */
+enum { HP_VARIANT_STENCIL = 0, HP_VARIANT_PENCIL = 1 };
+
+/* Select the sweep of hp_ppm_lxlylz, hp_evolve and the step pieces
+ * (default HP_VARIANT_STENCIL).  HP_ERR_UNSUPPORTED for a mixed-precision
+ * context or a z slab. */
+int hp_set_variant(hp_ctx *ctx, int variant);
+int hp_get_variant(hp_ctx *ctx);
+
+/* Attach the cho3d array ppm() reads at density peaks (ghosted host array,
+ * Fortran order, the shape of the state's arrays; hydropad/matrix.F90), or
+ * NULL for zeros (the default).  Uploaded once; the field is static. */
+int hp_attach_cho(hp_ctx *ctx, const double *cho3d, int nx, int ny, int nz,
+                  int nbound);
+
+/* Drop-in for the non-STENCIL ppmsolver (hydro/ppmsolver.F90:1-5 without
+ * STENCIL): one full-pencil sweep of the attached state in place, whatever
+ * hp_set_variant selected.  The host pointers identify the attached state
+ * as in hp_ppmsolver (cho3d: the attached one, or NULL); the *3dnew arrays
+ * are accepted and not written (the resident state is already the new one:
+ * a caller's savetn would copy stale host arrays, so drop it, and read the
+ * state back with hp_sync_to_host). */
+int hp_ppmsolver_pencil(hp_ctx *ctx, double *p3d, double *rho3d, double *vx3d,
+                        double *vy3d, double *vz3d, double *cho3d, double *nes3d,
+                        const double *gforce, double *p3dnew, double *rho3dnew,
+                        double *vx3dnew, double *vy3dnew, double *vz3dnew,
+                        double *cho3dnew, const int *nx, const int *ny,
+                        const int *nz, const int *nbound, const int *ndirection);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,5 +1,7 @@
 /*
- * hp_oracle.c -- CPU restatement of Hydropad's STENCIL PPM hydro step.
+ * hp_oracle.c -- CPU restatement of Hydropad's PPM hydro step: the STENCIL
+ * build's sweeps and, for parity with a non-STENCIL build, its full-pencil
+ * ppm() (hpo_ppmsolver_pencil).
  *
  * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline; never the
  * product).  PARITY UNPINNED against the Fortran reference: it cannot be
@@ -659,6 +661,303 @@ int hpo_ppmsolver(double *p3d, double *rho3d, double *vx3d, double *vy3d, double
 }
 
 /* ------------------------------------------------------------------ */
+/* hydro/flatten5.F90:1-40: flattening test of one variable over the   */
+/* four neighbour pairs of a 5-cell window.  When a pair's product is  */
+/* zero, gradleft is not assigned (:17-19): the reference's local is   */
+/* then stale or undefined; here it keeps its previous value (0 at the */
+/* start of the pencil), which adds nothing new to gradmax or the flag.*/
+/* ------------------------------------------------------------------ */
+static void flatten5(const double *abar, int *flatyn, double *gradleft, const hpo_scalars *s)
+{
+    double gradmax = 0.0;
+    for (int i = 1; i <= 4; ++i) {
+        const int ic = i + 1;
+        if (abar[ic] * abar[ic - 1] != 0.0)
+            *gradleft = fabs((abar[ic] - abar[ic - 1]) / fmin2(abar[ic], abar[ic - 1]));
+        gradmax = fmax2(gradmax, *gradleft);
+    }
+    if (gradmax >= s->mingradflat) *flatyn = 1;
+}
+
+typedef struct {
+    double jl[3], jr[3], d[3], a6[3];
+} pslot;
+
+static void pslot_shift(pslot *q)
+{
+    q->jl[1] = q->jl[2]; q->jr[1] = q->jr[2]; q->d[1] = q->d[2]; q->a6[1] = q->a6[2];
+}
+
+/* ------------------------------------------------------------------ */
+/* hydro/ppm.F90:1-662: one pencil of the non-STENCIL build.  Arrays   */
+/* are 1-based [1..ngrid], the whole gathered line with its ghosts;    */
+/* nmin = nbound, nmax = ngrid-nbound+1 (ppmsolver.F90:77-79).  pres.. */
+/* vz are updated in place over nmin..nmax as the reference does (the  */
+/* cells nmin and nmax are ghosts: they keep p and rho and get zero    */
+/* velocities, which the ghost fill after the sweep overwrites).       */
+/* Differences from the STENCIL path, all as in the reference:         */
+/*  - the characteristic speeds of cell k use the sound speed of cell  */
+/*    k+1 (cbar = c(i), c(i+1) with vxbar(2), vxbar(3) = cells i-1, i, */
+/*    :106-107; order2interp.F90:56-57 has c(i-1), c(i));              */
+/*  - the gravity parabola and ghalf are zero (:93,102);               */
+/*  - the density-peak fix sees cells i-2..i+1 along the sweep         */
+/*    (rhobar(1..4) of the 5-cell window);                             */
+/*  - pmean takes the cho-dependent values at density peaks (:585-594);*/
+/*  - the dual-energy switch divides by the largest new total energy   */
+/*    of the cell and its two neighbours, 0 beyond the line's updated  */
+/*    cells (:611-621).                                                */
+/* cho may be NULL (zeros).  A face that matches no wave pattern (NaN  */
+/* input) gets NaN, as in riemannsolver() here.  Returns the number of */
+/* Newton failures.                                                    */
+/* ------------------------------------------------------------------ */
+static int ppm_pencil(int ngrid, int nmin, int nmax, const double *cho, double *pres, double *rho,
+                      double *vx, double *vy, double *vz, const double *c, const double *eint,
+                      const double *etot, double *work, const hpo_scalars *s)
+{
+    const double gamma = s->gamma, rgamma1 = s->rgamma1, rdtath = s->rdtath, rdx = s->rdx, rat = s->rat;
+    const double mmmax = 0.0;
+    const size_t L = (size_t)ngrid + 2;
+    double *pnew = work, *rhonew = work + L, *vxnew = work + 2 * L, *vynew = work + 3 * L;
+    double *vznew = work + 4 * L, *etotnew = work + 5 * L, *eintnew = work + 6 * L;
+    memset(work, 0, 7 * L * sizeof(double));                               /* :64-71 */
+    pslot P, R, VX, VY, VZ;
+    memset(&P, 0, sizeof P); memset(&R, 0, sizeof R); memset(&VX, 0, sizeof VX);
+    memset(&VY, 0, sizeof VY); memset(&VZ, 0, sizeof VZ);
+    double pm[3] = {0, 0, 0}, rhom[3] = {0, 0, 0}, vxm[3] = {0, 0, 0}, vym[3] = {0, 0, 0}, vzm[3] = {0, 0, 0};
+    double gradleft = 0.0;
+    int fails = 0;
+    const int nmid = nmin + 1;
+    for (int i = nmin; i <= nmax; ++i) {
+        int flatyn = 0;
+        double flat = 0.0;
+        const int icell = i;
+        double pbar[6], rhobar[6], vxbar[6], vybar[6], vzbar[6], cbar[3];
+        for (int j = 1; j <= 5; ++j) {                                     /* :95-103 */
+            const int ia = icell + j - 3;
+            pbar[j] = pres[ia];
+            rhobar[j] = rho[ia];
+            vxbar[j] = vx[ia];
+            vybar[j] = vy[ia];
+            vzbar[j] = vz[ia];
+        }
+        cbar[1] = c[icell];
+        cbar[2] = c[icell + 1];
+        flatten5(pbar, &flatyn, &gradleft, s);                             /* :119-128 */
+        if (flatyn == 1) flat = s->flatvalue;
+        flatten5(rhobar, &flatyn, &gradleft, s);
+        if (flatyn == 1) flat = s->flatvalue;
+        flatten5(vxbar, &flatyn, &gradleft, s);
+        if (flatyn == 1) flat = s->flatvalue;
+        flatten5(vybar, &flatyn, &gradleft, s);
+        if (flatyn == 1) flat = s->flatvalue;
+        flatten5(vzbar, &flatyn, &gradleft, s);
+        if (flatyn == 1) flat = s->flatvalue;
+        pslot_shift(&P); pslot_shift(&R); pslot_shift(&VX); pslot_shift(&VY); pslot_shift(&VZ);  /* :138-165 */
+        const double addp = fabs(pbar[4] - pbar[2]) / fmin2(pbar[2], pbar[4]);             /* :169-171 */
+        const double addrho = 0.5 * gamma * fabs(rhobar[4] - rhobar[2]) / fmin2(rhobar[2], rhobar[4]);
+        double ptl, ptr, rhotl, rhotr, vxtl, vxtr, vytl, vytr, vztl, vztr;
+        double pcl[4], pcr[4], rhocl[4], rhocr[4], vxcl[4], vxcr[4], vycl[4], vycr[4], vzcl[4], vzcr[4];
+        correction(addp, addrho, pbar, P.jl, P.jr, P.d, P.a6, cbar, vxbar[2], vxbar[3], &ptl, &ptr, pcl, pcr,
+                   flat, 0, s);
+        correction(addp, addrho, rhobar, R.jl, R.jr, R.d, R.a6, cbar, vxbar[2], vxbar[3], &rhotl, &rhotr, rhocl,
+                   rhocr, flat, 1, s);
+        correction(addp, addrho, vxbar, VX.jl, VX.jr, VX.d, VX.a6, cbar, vxbar[2], vxbar[3], &vxtl, &vxtr, vxcl,
+                   vxcr, flat, 0, s);
+        correction(addp, addrho, vybar, VY.jl, VY.jr, VY.d, VY.a6, cbar, vxbar[2], vxbar[3], &vytl, &vytr, vycl,
+                   vycr, flat, 0, s);
+        correction(addp, addrho, vzbar, VZ.jl, VZ.jr, VZ.d, VZ.a6, cbar, vxbar[2], vxbar[3], &vztl, &vztr, vzcl,
+                   vzcr, flat, 0, s);
+        /* the g parabola of a zero gbar traces to exactly 0 (gcl = gcr = 0) */
+        if (ptl < 0.0) ptl = HPO_TINY;                                     /* :191-207 */
+        if (ptr < 0.0) ptr = HPO_TINY;
+        if (rhotl < 0.0) rhotl = HPO_TINY;
+        if (rhotr < 0.0) rhotr = HPO_TINY;
+        const double ctl = sqrt(gamma * ptl * rhotl);                      /* :209-210 */
+        const double ctr = sqrt(gamma * ptr * rhotr);
+        double lambdam = (vxbar[2] - cbar[1]) * rat, lambda0 = vxbar[2] * rat, lambdap = (vxbar[2] + cbar[1]) * rat;
+        double betaml, betapl, beta0l, betamr, betapr, beta0r, vyleft, vzleft, vyright, vzright;
+        betaml = (lambdam <= 0.0) ? 0.0 : beta(ctl, vxtl, vxcl[1], ptl, pcl[1], 0.0, -1.0, s);   /* :214-238 */
+        betapl = (lambdap <= 0.0) ? 0.0 : beta(ctl, vxtl, vxcl[3], ptl, pcl[3], 0.0, 1.0, s);
+        vyleft = vytl;
+        vzleft = vztl;
+        if (lambda0 <= 0.0) {
+            beta0l = 0.0;
+        } else {
+            beta0l = beta0(ctl, rhotl, rhocl[2], ptl, pcl[2], s);
+            vyleft = vycl[2];
+            vzleft = vzcl[2];
+        }
+        lambdam = (vxbar[3] - cbar[2]) * rat;                              /* :240-265 */
+        lambda0 = vxbar[3] * rat;
+        lambdap = (vxbar[3] + cbar[2]) * rat;
+        betapr = (lambdap >= 0.0) ? 0.0 : beta(ctr, vxtr, vxcr[3], ptr, pcr[3], 0.0, 1.0, s);
+        betamr = (lambdam >= 0.0) ? 0.0 : beta(ctr, vxtr, vxcr[1], ptr, pcr[1], 0.0, -1.0, s);
+        vyright = vytr;
+        vzright = vztr;
+        if (lambda0 >= 0.0) {
+            beta0r = 0.0;
+        } else {
+            beta0r = beta0(ctr, rhotr, rhocr[2], ptr, pcr[2], s);
+            vyright = vycr[2];
+            vzright = vzcr[2];
+        }
+        if (i == nmin) continue;                                           /* :267 */
+        double pleft = ptl + ctl * ctl * (betapl + betaml);                /* :269-278 */
+        if (pleft <= 0.0) pleft = ptl;
+        double pright = ptr + ctr * ctr * (betapr + betamr);
+        if (pright <= 0.0) pright = ptr;
+        const double vxleft = vxtl + ctl * (betapl - betaml);
+        const double vxright = vxtr + ctr * (betapr - betamr);
+        double rholeft = 1.0 / (1.0 / rhotl - betaml - beta0l - betapl);
+        if (rholeft <= 0.0) rholeft = rhotl;
+        double rhoright = 1.0 / (1.0 / rhotr - betamr - beta0r - betapr);
+        if (rhoright <= 0.0) rhoright = rhotr;
+        pm[1] = pm[2];                                                     /* :310-314 */
+        rhom[1] = rhom[2];
+        vxm[1] = vxm[2];
+        vym[1] = vym[2];
+        vzm[1] = vzm[2];
+        /* :279-531: the classification and the four wave patterns, the
+         * transverse upwinding and the density-peak fix are riemannsolver's
+         * (the same statements), with rhobar/vxbar of this 5-cell window */
+        fails += riemannsolver(rhobar, vxbar, pleft, pright, rholeft, rhoright, vxleft, vxright, vyleft, vyright,
+                               vzleft, vzright, &pm[2], &rhom[2], &vxm[2], &vym[2], &vzm[2], s);
+        if (i == nmid) continue;                                           /* :534-535 */
+        const int index = icell - 1;                                       /* :544-606 */
+        double flux1 = rhom[1] * vxm[1], flux2 = rhom[2] * vxm[2];
+        rhonew[index] = rho[index] + rdtath * (flux1 - flux2) * rdx;
+        /* grav = (rhoold1d + rhonew) * ghalf * 0.5 with ghalf = 0 (:93): no term */
+        flux1 = rhom[1] * vxm[1] * vxm[1] + pm[1];
+        flux2 = rhom[2] * vxm[2] * vxm[2] + pm[2];
+        vxnew[index] = (vx[index] * rho[index] + rdtath * (flux1 - flux2) * rdx) / rhonew[index];
+        flux1 = vym[1] * vxm[1] * rhom[1];
+        flux2 = vym[2] * vxm[2] * rhom[2];
+        vynew[index] = (rho[index] * vy[index] + rdtath * (flux1 - flux2) * rdx) / rhonew[index];
+        flux1 = vzm[1] * vxm[1] * rhom[1];
+        flux2 = vzm[2] * vxm[2] * rhom[2];
+        vznew[index] = (rho[index] * vz[index] + rdtath * (flux1 - flux2) * rdx) / rhonew[index];
+        flux1 = (gamma * pm[1] * rgamma1 + 0.5 * rhom[1] * (vxm[1] * vxm[1] + vym[1] * vym[1] + vzm[1] * vzm[1])) * vxm[1];
+        flux2 = (gamma * pm[2] * rgamma1 + 0.5 * rhom[2] * (vxm[2] * vxm[2] + vym[2] * vym[2] + vzm[2] * vzm[2])) * vxm[2];
+        etotnew[index] = etot[index] + rdtath * (flux1 - flux2) * rdx;
+        double pmean = (pm[1] + pm[2]) * 0.5;
+        if (rhobar[2] > s->dmax * rhobar[1] && rhobar[2] > s->dmax * rhobar[3]) {
+            const double ch = cho ? cho[index] : 0.0;
+            if (ch == 1.0) {
+                const double maxp = (vxm[1] - vxm[2]) * rhobar[2] * fmax2(mmmax, vxm[1] - vxm[2]);
+                pmean = fmax2(pmean, maxp);
+            } else if (ch == 2.0) {
+                pmean = (gamma - 1.0) * eint[index];
+            }
+        }
+        eintnew[index] = eint[index] + rdtath * pmean * (vxm[1] - vxm[2]) * rdx;
+        flux1 = (pm[1] * vxm[1]) * rgamma1;
+        flux2 = (pm[2] * vxm[2]) * rgamma1;
+        eintnew[index] = eintnew[index] + rdtath * (flux1 - flux2) * rdx;
+        if (eintnew[index] < 0.0) eintnew[index] = eint[index];
+    }
+    for (int i = nmin; i <= nmax; ++i) {                                   /* :611-638 */
+        double eeleft = etotnew[i - 1];
+        if (i == nmin) eeleft = 0.0;
+        const double ee = etotnew[i];
+        double eeright = etotnew[i + 1];
+        if (i == nmax) eeright = 0.0;
+        const double ee2 = fmax2(fmax2(eeleft, ee), eeright);
+        const double vvv = vxnew[i] * vxnew[i] + vynew[i] * vynew[i] + vznew[i] * vznew[i];
+        const double eeaux = etotnew[i] - 0.5 * rhonew[i] * vvv;
+        const double ee1 = eeaux / ee2;
+        if (ee1 >= s->eta2) eintnew[i] = eeaux;
+        const double ee0 = eeaux / etotnew[i];
+        if (ee0 >= s->eta1) pnew[i] = (gamma - 1.0) * eeaux;
+        else pnew[i] = (gamma - 1.0) * eintnew[i];
+    }
+    for (int i = nmin; i <= nmax; ++i) {                                   /* :646-658 */
+        if (eintnew[i] <= 0.0) {
+            eintnew[i] = eint[i];
+            pnew[i] = pres[i];
+        }
+        if (rhonew[i] <= 0.0) rhonew[i] = rho[i];
+        pres[i] = pnew[i];
+        rho[i] = rhonew[i];
+        vx[i] = vxnew[i];
+        vy[i] = vynew[i];
+        vz[i] = vznew[i];
+    }
+    return fails;
+}
+
+/* ppmsolver.F90:162-190, 290-318, 418-446 (#else of STENCIL) and
+ * hydropad/savetn.F90: every interior pencil is gathered whole (ghosts
+ * included), solved by ppm_pencil, scattered into the new arrays, which
+ * then replace the state. */
+int hpo_ppmsolver_pencil(double *p3d, double *rho3d, double *vx3d, double *vy3d, double *vz3d,
+                         const double *cho3d, int nx, int ny, int nz, int nbound, int ndirection,
+                         const hpo_scalars *s, int nthreads)
+{
+    const size_t ncell = (size_t)nx * ny * nz;
+    double *old[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
+    double *nw[5];
+    for (int q = 0; q < 5; ++q) {
+        /* the new arrays keep their contents outside the solved pencils
+         * (ghost pencils), which the ghost fill after the sweep replaces */
+        nw[q] = malloc(ncell * sizeof(double));
+        memcpy(nw[q], old[q], ncell * sizeof(double));
+    }
+    const int ngrid = (ndirection == 1) ? nx : (ndirection == 2) ? ny : nz;
+    const int nmin = nbound, nmax = ngrid - nbound + 1;
+    const int t1max = (ndirection == 1) ? ny : nx;
+    const int t2max = (ndirection == 3) ? ny : nz;
+    int fails = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#define CELL(ia, t1, t2) ((ndirection == 1) ? IX((ia), (t1), (t2)) : (ndirection == 2) ? IX((t1), (ia), (t2)) : IX((t1), (t2), (ia)))
+#pragma omp parallel reduction(+ : fails)
+    {
+        const size_t L = (size_t)ngrid + 2;
+        double *buf = malloc(17 * L * sizeof(double));
+        double *pres = buf, *rho = buf + L, *vx = buf + 2 * L, *vy = buf + 3 * L, *vz = buf + 4 * L;
+        double *c = buf + 5 * L, *eint = buf + 6 * L, *etot = buf + 7 * L, *cho = buf + 8 * L;
+        double *work = buf + 9 * L;
+        memset(buf, 0, 9 * L * sizeof(double));
+#pragma omp for collapse(2) schedule(static)
+        for (int t2 = nbound + 1; t2 <= t2max - nbound; ++t2) {
+            for (int t1 = nbound + 1; t1 <= t1max - nbound; ++t1) {
+                for (int i = 1; i <= ngrid; ++i) {
+                    const size_t q = CELL(i, t1, t2);
+                    pres[i] = p3d[q];
+                    rho[i] = rho3d[q];
+                    if (ndirection == 1) { vx[i] = vx3d[q]; vy[i] = vy3d[q]; vz[i] = vz3d[q]; }
+                    else if (ndirection == 2) { vx[i] = vy3d[q]; vy[i] = vx3d[q]; vz[i] = vz3d[q]; }
+                    else { vx[i] = vz3d[q]; vy[i] = vy3d[q]; vz[i] = vx3d[q]; }
+                    eint[i] = internal(pres[i], s);
+                    etot[i] = total(pres[i], rho[i], vx[i], vy[i], vz[i], s);
+                    cho[i] = cho3d ? cho3d[q] : 0.0;
+                    c[i] = sqrt(s->gamma * p3d[q] / rho3d[q]);
+                }
+                fails += ppm_pencil(ngrid, nmin, nmax, cho, pres, rho, vx, vy, vz, c, eint, etot, work, s);
+                for (int i = 1; i <= ngrid; ++i) {
+                    const size_t q = CELL(i, t1, t2);
+                    nw[0][q] = pres[i];
+                    nw[1][q] = rho[i];
+                    if (ndirection == 1) { nw[2][q] = vx[i]; nw[3][q] = vy[i]; nw[4][q] = vz[i]; }
+                    else if (ndirection == 2) { nw[3][q] = vx[i]; nw[2][q] = vy[i]; nw[4][q] = vz[i]; }
+                    else { nw[4][q] = vx[i]; nw[3][q] = vy[i]; nw[2][q] = vz[i]; }
+                }
+            }
+        }
+        free(buf);
+    }
+#undef CELL
+    for (int q = 0; q < 5; ++q) {                                          /* savetn.F90:11-21 */
+        memcpy(old[q], nw[q], ncell * sizeof(double));
+        free(nw[q]);
+    }
+    return fails;
+}
+
+/* ------------------------------------------------------------------ */
 /* Ghost fill: exchange_mesh with one rank, periodic in every axis     */
 /* (exchange_mesh.F90:23-41 + exchange_var.F90:19-53, neighbours=self) */
 /* ------------------------------------------------------------------ */
@@ -704,8 +1003,12 @@ int hpo_ppm_lxlylz(double *p3d, double *rho3d, double *vx3d, double *vy3d, doubl
     static const int order[6][3] = {{1, 2, 3}, {3, 2, 1}, {2, 3, 1}, {1, 3, 2}, {3, 1, 2}, {2, 1, 3}};
     int fails = 0;
     for (int k = 0; k < 3; ++k) {
-        fails += hpo_ppmsolver(p3d, rho3d, vx3d, vy3d, vz3d, gforce, nx, ny, nz, nbound, order[nrot - 1][k], s,
-                               nthreads);
+        if (s->pencil)  /* the non-STENCIL build (cho3d of the hydro-only runs: zeros) */
+            fails += hpo_ppmsolver_pencil(p3d, rho3d, vx3d, vy3d, vz3d, NULL, nx, ny, nz, nbound,
+                                          order[nrot - 1][k], s, nthreads);
+        else
+            fails += hpo_ppmsolver(p3d, rho3d, vx3d, vy3d, vz3d, gforce, nx, ny, nz, nbound, order[nrot - 1][k],
+                                   s, nthreads);
         hpo_exchange_mesh(p3d, rho3d, vx3d, vy3d, vz3d, nx, ny, nz, nbound);
     }
     return fails;

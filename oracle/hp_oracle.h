@@ -39,7 +39,8 @@ typedef struct {
     int    cosmo;    /* 1: EdS expanding background (timedet_cosmo + expand) */
     int    expand_zero_old; /* 1: expand with vxold=pold3d=0 (non-STENCIL allocation);
                                0: snapshot of v,p at step start */
-    int    pad;
+    int    pencil;   /* 0: STENCIL sweeps (ppmsolver.F90 #ifdef STENCIL branches);
+                        1: the non-STENCIL build's full-pencil ppm() (hydro/ppm.F90) */
 } hpo_scalars;
 
 /* Derived constants from gamma, N (initialize_parameters.F90:23-24,63-69). */
@@ -56,6 +57,16 @@ int hpo_ppmsolver(double *p3d, double *rho3d, double *vx3d, double *vy3d,
 
 /* Periodic ghost fill for one process (exchange_mesh.F90 / exchange_var.F90
  * with npes=1: every Cartesian neighbour is this rank). */
+/* One sweep of the non-STENCIL build (ppmsolver.F90:162-190, 290-318,
+ * 418-446 -> hydro/ppm.F90 per pencil, then savetn): the same arrays and
+ * arguments as hpo_ppmsolver; cho3d (ghosted, or NULL for zeros) is the
+ * cho3d array that ppm() reads at density peaks.  The gravity source is
+ * ignored, as ppm() zeroes it (ppm.F90:93,102). */
+int hpo_ppmsolver_pencil(double *p3d, double *rho3d, double *vx3d, double *vy3d,
+                         double *vz3d, const double *cho3d, int nx, int ny, int nz,
+                         int nbound, int ndirection, const hpo_scalars *s,
+                         int nthreads);
+
 void hpo_exchange_mesh(double *p3d, double *rho3d, double *vx3d, double *vy3d,
                        double *vz3d, int nx, int ny, int nz, int nbound);
 

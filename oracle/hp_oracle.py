@@ -32,7 +32,7 @@ class HpoScalars(C.Structure):
         "dt", "rdtath", "at", "dat", "rat", "ath", "dath",
         "t", "told", "thalf", "dtold", "tstop", "atnew", "datnew",
         "dt_cap", "velmax")] + [
-        ("nstep", C.c_int), ("cosmo", C.c_int), ("expand_zero_old", C.c_int), ("pad", C.c_int)]
+        ("nstep", C.c_int), ("cosmo", C.c_int), ("expand_zero_old", C.c_int), ("pencil", C.c_int)]
 
 
 def build() -> str:
@@ -58,6 +58,8 @@ def lib():
         L.hpo_derive_constants.argtypes = [sp, C.c_double, C.c_int]
         L.hpo_ppmsolver.argtypes = [dp] * 5 + [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, sp, C.c_int]
         L.hpo_ppmsolver.restype = C.c_int
+        L.hpo_ppmsolver_pencil.argtypes = [dp] * 5 + [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, sp, C.c_int]
+        L.hpo_ppmsolver_pencil.restype = C.c_int
         L.hpo_exchange_mesh.argtypes = [dp] * 5 + [C.c_int] * 4
         L.hpo_ppm_lxlylz.argtypes = [dp] * 5 + [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, sp, C.c_int]
         L.hpo_ppm_lxlylz.restype = C.c_int
@@ -103,10 +105,12 @@ def make_scalars(params) -> HpoScalars:
 class OracleState:
     """Ghosted Fortran-order state (p, rho, vx, vy, vz) driven by the oracle."""
 
-    def __init__(self, p, rho, vx, vy, vz, nbound=3, gforce=None):
+    def __init__(self, p, rho, vx, vy, vz, nbound=3, gforce=None, cho=None):
         self.f = [np.array(a, dtype=np.float64, order="F", copy=True) for a in (p, rho, vx, vy, vz)]
         self.nbound = nbound
         self.gforce = None if gforce is None else np.asfortranarray(gforce, dtype=np.float64)
+        # cho3d of the non-STENCIL build's pencil solver (ghosted), or None (zeros)
+        self.cho = None if cho is None else np.asfortranarray(cho, dtype=np.float64)
         self.nx, self.ny, self.nz = self.f[0].shape
 
     @property
@@ -123,6 +127,12 @@ class OracleState:
     def ppmsolver(self, s: HpoScalars, ndirection: int, nthreads: int = 0) -> int:
         return lib().hpo_ppmsolver(*[_ptr(a) for a in self.f], _ptr(self.gforce), self.nx, self.ny,
                                    self.nz, self.nbound, ndirection, C.byref(s), nthreads)
+
+    def ppmsolver_pencil(self, s: HpoScalars, ndirection: int, nthreads: int = 0) -> int:
+        """One sweep of the non-STENCIL build (ppm() per pencil + savetn);
+        the ghost fill that ppm_lxlylz does after it is left to the caller."""
+        return lib().hpo_ppmsolver_pencil(*[_ptr(a) for a in self.f], _ptr(self.cho), self.nx, self.ny,
+                                          self.nz, self.nbound, ndirection, C.byref(s), nthreads)
 
     def ppm_lxlylz(self, s: HpoScalars, nrot: int, nthreads: int = 0) -> int:
         return lib().hpo_ppm_lxlylz(*[_ptr(a) for a in self.f], _ptr(self.gforce), self.nx, self.ny,

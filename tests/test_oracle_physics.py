@@ -114,3 +114,71 @@ def test_newton_cap_reported(oracle):
     s = oracle.make_scalars(params_for((n, n, n)))
     oracle_first_dt(oracle, st, s)
     assert st.ppmsolver(s, 1) == 0
+
+
+# ---- the non-STENCIL build's full-pencil solver (hydro/ppm.F90) ----------
+
+def _pencil_run(oracle, state, prm, steps):
+    st = oracle.OracleState(*state)
+    s = oracle.make_scalars(prm)
+    s.pencil = 1
+    oracle_first_dt(oracle, st, s)
+    assert st.evolve(s, steps) == 0
+    return st, s
+
+
+def test_pencil_uniform_state_is_steady(oracle):
+    n = 10
+    shape = (n + 2 * NB,) * 3
+    one = np.ones(shape, order="F")
+    state = (0.6 * one, 1.3 * one, 0.2 * one, -0.1 * one, 0.05 * one)
+    st, _ = _pencil_run(oracle, state, params_for((n, n, n)), 3)
+    for q in range(5):
+        assert np.array_equal(interior(st.f[q]), interior(state[q])), q
+
+
+def test_pencil_conservation_periodic(oracle):
+    """Mass and momentum to round-off, at Courant number 0.3: on this rough
+    field the full-pencil solver's characteristic speeds (the next cell's
+    sound speed) drive a few densities negative from 0.5 up, and the
+    reference's fallback (keep the old density, ppm.F90:651) then does not
+    conserve mass; the STENCIL sweep stays positive at 0.8."""
+    n = 12
+    state = grf_state(n, seed=4)
+    st, _ = _pencil_run(oracle, state, params_for((n, n, n), cour=0.3), 4)
+    r0, r1 = interior(state[1]), interior(st.rho)
+    assert abs(r1.sum() - r0.sum()) <= 1e-12 * r0.sum()
+    for q in (2, 3, 4):
+        m0 = (r0 * interior(state[q])).sum()
+        m1 = (r1 * interior(st.f[q])).sum()
+        assert abs(m1 - m0) <= 1e-11 * np.abs(r0 * interior(state[q])).sum()
+
+
+def test_pencil_sound_speed_of_next_cell(oracle):
+    """The only tracing difference from the STENCIL sweep is the sound speed
+    of the characteristic speeds (cell k takes cell k+1's, ppm.F90:106-107):
+    with a uniform sound speed (the isothermal GRF) and no density peak the
+    two sweeps give the same bits; with a varying one they differ."""
+    n = 12
+    state = grf_state(n, seed=8)
+    prm = params_for((n, n, n), cosmo=True)
+    outs = []
+    for pencil in (False, True):
+        st = oracle.OracleState(*state)
+        s = oracle.make_scalars(prm)
+        oracle_first_dt(oracle, st, s)
+        (st.ppmsolver_pencil if pencil else st.ppmsolver)(s, 1)
+        outs.append([interior(a).copy() for a in st.f])
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    warm = oracle.OracleState(*state)
+    warm.f[0][...] *= 1.0 + 0.5 * np.random.default_rng(3).random(warm.f[0].shape)
+    warm.exchange()
+    outs = []
+    for pencil in (False, True):
+        st = oracle.OracleState(*warm.f)
+        s = oracle.make_scalars(prm)
+        oracle_first_dt(oracle, st, s)
+        (st.ppmsolver_pencil if pencil else st.ppmsolver)(s, 1)
+        outs.append(interior(st.f[1]).copy())
+    assert not np.array_equal(outs[0], outs[1])
