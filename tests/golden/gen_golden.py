@@ -1,5 +1,6 @@
-"""Second, independent restatement of the STENCIL ppmsolver in plain Python,
-used to generate golden vectors that pin the C oracle.
+"""Second, independent restatement of the STENCIL ppmsolver (and of the
+non-STENCIL build's full-pencil ppm()) in plain Python, used to generate
+golden vectors that pin the C oracle.
 
 The reference (Fortran 90 + OpenACC) cannot be compiled here and ships no
 test vectors, so this file transliterates the same routines a second time,
@@ -12,7 +13,8 @@ Fortran indices to keep the transliteration literal.
 
 Sources: hydro/ppmsolver.F90:96-160,214-288,342-416; order2interp.F90;
 ppm_functs.F90; dda.F90; riemannsolver.F90; riemann.F90; integrate.F90;
-total.F90; internal.F90.
+total.F90; internal.F90; for the pencil cases ppm.F90, flatten5.F90 and
+ppmsolver.F90:162-190,290-318,418-446.
 """
 from __future__ import annotations
 
@@ -468,11 +470,193 @@ def ppmsolver(F, nb, nd, S, G=None):
     return [out_p, out_r, out_u, out_v, out_w]
 
 
+# ---------------------------------------------------------------------------
+# The non-STENCIL build's full-pencil solver: hydro/ppm.F90 per pencil (with
+# flatten5.F90), called by ppmsolver.F90:162-190, 290-318, 418-446 on whole
+# gathered lines, then savetn.  Transliterated a second time from the
+# Fortran, independently of oracle/hp_oracle.c.
+# ---------------------------------------------------------------------------
+def flatten5(abar, keep, S):
+    """flatten5.F90: 1 when the largest relative jump of the 4 pairs
+    reaches mingradflat.  A zero product leaves gradleft as it was (kept in
+    keep['g'] across calls; 0 at the start of the pencil)."""
+    gradmax = 0.0
+    for i in range(1, 5):
+        ic = i + 1
+        if abar[ic] * abar[ic - 1] != 0.0:
+            keep["g"] = abs((abar[ic] - abar[ic - 1]) / MIN(abar[ic], abar[ic - 1]))
+        gradmax = MAX(gradmax, keep["g"])
+    return 1 if gradmax >= S.mingradflat else 0
+
+
+def ppm_pencil(pres, rho, vx, vy, vz, c, eint, etot, cho, ngrid, nb, S):
+    """ppm.F90:1-662 on one gathered line (1-based dicts over 1..ngrid);
+    returns the line's new p, rho, vx, vy, vz (dicts) as the reference
+    leaves them (cells nmin..nmax written)."""
+    nmin, nmax = nb, ngrid - nb + 1
+    nmid = nmin + 1
+    z = {i: np.float64(0.0) for i in range(0, ngrid + 2)}  # IEEE division (0/0 -> NaN) at the ghosts
+    pnew, rhonew, vxnew, vynew, vznew, etotnew, eintnew = (dict(z) for _ in range(7))
+    z0 = np.float64(0.0)
+    slots = [tuple({1: z0, 2: z0} for _ in range(4)) for _ in range(5)]
+    face = {1: (0.0,) * 5, 2: (0.0,) * 5}
+    keep = {"g": 0.0}
+    for i in range(nmin, nmax + 1):
+        flatyn, flat = 0, 0.0
+        bars = [{j: arr[i + j - 3] for j in range(1, 6)} for arr in (pres, rho, vx, vy, vz)]
+        pbar, rhobar, vxbar, vybar, vzbar = bars
+        cbar = {1: c[i], 2: c[i + 1]}              # ppm.F90:106-107
+        for arr in bars:
+            if flatten5(arr, keep, S):
+                flatyn = 1
+            if flatyn == 1:
+                flat = S.flatvalue
+        for sl4 in slots:
+            for sl in sl4:
+                sl[1] = sl[2]
+        addp = abs(pbar[4] - pbar[2]) / MIN(pbar[2], pbar[4])
+        addrho = 0.50 * S.gamma * abs(rhobar[4] - rhobar[2]) / MIN(rhobar[2], rhobar[4])
+        res = [correction(addp, addrho, arr, *slots[k], cbar, vxbar[2], vxbar[3], flat, nd, S)
+               for k, (arr, nd) in enumerate(((pbar, 0), (rhobar, 1), (vxbar, 0), (vybar, 0), (vzbar, 0)))]
+        (ptl, ptr, pcl, pcr), (rhotl, rhotr, rhocl, rhocr), (vxtl, vxtr, vxcl, vxcr) = res[0], res[1], res[2]
+        (vytl, vytr, vycl, vycr), (vztl, vztr, vzcl, vzcr) = res[3], res[4]
+        if ptl < 0.0:
+            ptl = TINY
+        if ptr < 0.0:
+            ptr = TINY
+        if rhotl < 0.0:
+            rhotl = TINY
+        if rhotr < 0.0:
+            rhotr = TINY
+        ctl = np.sqrt(S.gamma * ptl * rhotl)
+        ctr = np.sqrt(S.gamma * ptr * rhotr)
+        lm, l0, lp = (vxbar[2] - cbar[1]) * S.rat, vxbar[2] * S.rat, (vxbar[2] + cbar[1]) * S.rat
+        betaml = 0.0 if lm <= 0.0 else beta(ctl, vxtl, vxcl[1], ptl, pcl[1], 0.0, -1.0, S)
+        betapl = 0.0 if lp <= 0.0 else beta(ctl, vxtl, vxcl[3], ptl, pcl[3], 0.0, 1.0, S)
+        vyleft, vzleft = vytl, vztl
+        if l0 <= 0.0:
+            beta0l = 0.0
+        else:
+            beta0l = beta0(ctl, rhotl, rhocl[2], ptl, pcl[2], S)
+            vyleft, vzleft = vycl[2], vzcl[2]
+        lm, l0, lp = (vxbar[3] - cbar[2]) * S.rat, vxbar[3] * S.rat, (vxbar[3] + cbar[2]) * S.rat
+        betapr = 0.0 if lp >= 0.0 else beta(ctr, vxtr, vxcr[3], ptr, pcr[3], 0.0, 1.0, S)
+        betamr = 0.0 if lm >= 0.0 else beta(ctr, vxtr, vxcr[1], ptr, pcr[1], 0.0, -1.0, S)
+        vyright, vzright = vytr, vztr
+        if l0 >= 0.0:
+            beta0r = 0.0
+        else:
+            beta0r = beta0(ctr, rhotr, rhocr[2], ptr, pcr[2], S)
+            vyright, vzright = vycr[2], vzcr[2]
+        if i == nmin:
+            continue
+        pleft = ptl + ctl * ctl * (betapl + betaml)
+        if pleft <= 0.0:
+            pleft = ptl
+        pright = ptr + ctr * ctr * (betapr + betamr)
+        if pright <= 0.0:
+            pright = ptr
+        vxleft = vxtl + ctl * (betapl - betaml)
+        vxright = vxtr + ctr * (betapr - betamr)
+        rholeft = 1.0 / (1.0 / rhotl - betaml - beta0l - betapl)
+        if rholeft <= 0.0:
+            rholeft = rhotl
+        rhoright = 1.0 / (1.0 / rhotr - betamr - beta0r - betapr)
+        if rhoright <= 0.0:
+            rhoright = rhotr
+        face[1] = face[2]
+        face[2] = riemannsolver(rhobar, vxbar, pleft, pright, rholeft, rhoright, vxleft, vxright, vyleft, vyright,
+                                vzleft, vzright, S)
+        if i == nmid:
+            continue
+        (pm1, rhom1, vxm1, vym1, vzm1), (pm2, rhom2, vxm2, vym2, vzm2) = face[1], face[2]
+        ix = i - 1
+        rhonew[ix] = rho[ix] + S.rdtath * (rhom1 * vxm1 - rhom2 * vxm2) * S.rdx
+        fl1, fl2 = rhom1 * vxm1 * vxm1 + pm1, rhom2 * vxm2 * vxm2 + pm2
+        vxnew[ix] = (vx[ix] * rho[ix] + S.rdtath * (fl1 - fl2) * S.rdx) / rhonew[ix]
+        fl1, fl2 = vym1 * vxm1 * rhom1, vym2 * vxm2 * rhom2
+        vynew[ix] = (rho[ix] * vy[ix] + S.rdtath * (fl1 - fl2) * S.rdx) / rhonew[ix]
+        fl1, fl2 = vzm1 * vxm1 * rhom1, vzm2 * vxm2 * rhom2
+        vznew[ix] = (rho[ix] * vz[ix] + S.rdtath * (fl1 - fl2) * S.rdx) / rhonew[ix]
+        g = S.gamma
+        fl1 = (g * pm1 * S.rgamma1 + 0.50 * rhom1 * (vxm1 * vxm1 + vym1 * vym1 + vzm1 * vzm1)) * vxm1
+        fl2 = (g * pm2 * S.rgamma1 + 0.50 * rhom2 * (vxm2 * vxm2 + vym2 * vym2 + vzm2 * vzm2)) * vxm2
+        etotnew[ix] = etot[ix] + S.rdtath * (fl1 - fl2) * S.rdx
+        pmean = (pm1 + pm2) * 0.5
+        if rhobar[2] > S.dmax * rhobar[1] and rhobar[2] > S.dmax * rhobar[3]:
+            if cho[ix] == 1.0:
+                pmean = MAX(pmean, (vxm1 - vxm2) * rhobar[2] * MAX(0.0, vxm1 - vxm2))
+            elif cho[ix] == 2.0:
+                pmean = (g - 1.0) * eint[ix]
+        eintnew[ix] = eint[ix] + S.rdtath * pmean * (vxm1 - vxm2) * S.rdx
+        fl1, fl2 = (pm1 * vxm1) * S.rgamma1, (pm2 * vxm2) * S.rgamma1
+        eintnew[ix] = eintnew[ix] + S.rdtath * (fl1 - fl2) * S.rdx
+        if eintnew[ix] < 0:
+            eintnew[ix] = eint[ix]
+    for i in range(nmin, nmax + 1):
+        eeleft = 0.0 if i == nmin else etotnew[i - 1]
+        eeright = 0.0 if i == nmax else etotnew[i + 1]
+        ee2 = MAX(eeleft, etotnew[i], eeright)
+        vvv = vxnew[i] * vxnew[i] + vynew[i] * vynew[i] + vznew[i] * vznew[i]
+        eeaux = etotnew[i] - 0.50 * rhonew[i] * vvv
+        if eeaux / ee2 >= S.eta2:
+            eintnew[i] = eeaux
+        if eeaux / etotnew[i] >= S.eta1:
+            pnew[i] = (S.gamma - 1) * eeaux
+        else:
+            pnew[i] = (S.gamma - 1) * eintnew[i]
+    out = [dict(pres), dict(rho), dict(vx), dict(vy), dict(vz)]
+    for i in range(nmin, nmax + 1):
+        if eintnew[i] <= 0.0:
+            pnew[i] = pres[i]
+        if rhonew[i] <= 0.0:
+            rhonew[i] = rho[i]
+        out[0][i], out[1][i], out[2][i], out[3][i], out[4][i] = pnew[i], rhonew[i], vxnew[i], vynew[i], vznew[i]
+    return out
+
+
+def ppmsolver_pencil(F, nb, nd, S, cho3d):
+    """One non-STENCIL sweep of the ghosted fields F (savetn included)."""
+    p3d, r3d, u3d, v3d, w3d = [a.copy(order="F") for a in F]
+    nx, ny, nz = p3d.shape
+    A = lambda arr, i, j, k: arr[i - 1, j - 1, k - 1]
+    if nd == 1:
+        ns, t1r, t2r, cell, roles = nx, range(nb + 1, ny - nb + 1), range(nb + 1, nz - nb + 1), \
+            (lambda s, a, b: (s, a, b)), (0, 1, 2)
+    elif nd == 2:
+        ns, t1r, t2r, cell, roles = ny, range(nb + 1, nx - nb + 1), range(nb + 1, nz - nb + 1), \
+            (lambda s, a, b: (a, s, b)), (1, 0, 2)
+    else:
+        ns, t1r, t2r, cell, roles = nz, range(nb + 1, nx - nb + 1), range(nb + 1, ny - nb + 1), \
+            (lambda s, a, b: (a, b, s)), (2, 1, 0)
+    vel = (u3d, v3d, w3d)
+    new = [a.copy(order="F") for a in (p3d, r3d, u3d, v3d, w3d)]
+    for b in t2r:
+        for a in t1r:
+            pres, rho, vx, vy, vz, c, eint, etot, cho = ({} for _ in range(9))
+            for i in range(1, ns + 1):
+                q = cell(i, a, b)
+                pres[i], rho[i] = A(p3d, *q), A(r3d, *q)
+                vx[i], vy[i], vz[i] = (A(vel[r], *q) for r in roles)
+                eint[i] = pres[i] * S.rgamma1
+                etot[i] = pres[i] * S.rgamma1 + 0.5 * rho[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i])
+                cho[i] = A(cho3d, *q)
+                c[i] = np.sqrt(S.gamma * pres[i] / rho[i])
+            c[ns + 1] = np.float64(0.0)  # never read (cbar(2) of i = nmax <= ns)
+            res = ppm_pencil(pres, rho, vx, vy, vz, c, eint, etot, cho, ns, nb, S)
+            for i in range(1, ns + 1):
+                idx = tuple(x - 1 for x in cell(i, a, b))
+                new[0][idx], new[1][idx] = res[0][i], res[1][i]
+                for r, f in zip(roles, (res[2], res[3], res[4])):
+                    new[2 + r][idx] = f[i]
+    return new
+
+
 def _ghost(a, nb):
     return np.asfortranarray(np.pad(a, nb, mode="wrap"))
 
 
-def make_case(seed, n=(10, 8, 6), nb=3, peak=False):
+def make_case(seed, n=(10, 8, 6), nb=3, peak=False, single=False):
     rng = np.random.Generator(np.random.PCG64(seed))
     shape = tuple(n)
     x = np.linspace(0, 2 * np.pi, shape[0], endpoint=False)[:, None, None]
@@ -481,6 +665,8 @@ def make_case(seed, n=(10, 8, 6), nb=3, peak=False):
     if peak:
         rho[3::5, :, :] *= 40.0  # two-cell density spikes along x
         rho[4::5, :, :] *= 40.0
+    if single:
+        rho[6::10, :, :] *= 40.0  # one-cell spikes along x (a peak above both neighbours)
     vel = [0.6 * rng.standard_normal(shape) for _ in range(3)]
     vel[1][:, ::3, :] = 0.0  # exact zeros exercise the stale-gradleft path
     return [_ghost(a, nb) for a in (p, rho, *vel)]
@@ -499,6 +685,12 @@ CASES = [
     ("grav_x", 7, (10, 8, 6), 1, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
     ("grav_y", 8, (8, 10, 6), 2, dict(dt=1.5e-3, at=0.05, dat=3.1, ath=0.0502), dict()),
     ("grav_z", 9, (6, 8, 10), 3, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
+    # the non-STENCIL build's full-pencil solver; pencil_peak_x: density spikes
+    # along the sweep with dmax = 2 and a cho3d of 0, 1, 2
+    ("pencil_x", 10, (10, 8, 6), 1, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
+    ("pencil_y", 11, (8, 10, 6), 2, dict(dt=1.5e-3, at=0.05, dat=3.1, ath=0.0502), dict()),
+    ("pencil_z", 12, (6, 8, 10), 3, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
+    ("pencil_peak_x", 13, (10, 8, 6), 1, dict(dt=1e-3, at=1.0, dat=0.0, ath=1.0), dict(dmax=2.0)),
 ]
 
 
@@ -517,11 +709,15 @@ def gravity_field(shape, nb, alpha=40.0, sigma=0.3):
 
 def run_case(name, seed, shape, nd, tsc, extra):
     nb = 3
-    F = make_case(seed, shape, nb, peak=name.startswith("peak"))
+    F = make_case(seed, shape, nb, peak="peak" in name, single=name == "pencil_peak_x")
     S = Sc(5.0 / 3.0, 1.0 / max(shape), **tsc, **extra)
     G = gravity_field(shape, nb) if name.startswith("grav") else None
+    if name.startswith("pencil"):
+        rng = np.random.Generator(np.random.PCG64(seed + 100))
+        cho = _ghost(rng.integers(0, 3, shape).astype(np.float64), nb)
+        return F, ppmsolver_pencil(F, nb, nd, S, cho), S, {"cho": cho}
     out = ppmsolver(F, nb, nd, S, G)
-    return F, out, S, G
+    return F, out, S, ({} if G is None else {"gforce": G})
 
 
 def main(names=None):
@@ -531,8 +727,7 @@ def main(names=None):
     for name, seed, shape, nd, tsc, extra in CASES:
         if names and name not in names:
             continue
-        F, out, S, G = run_case(name, seed, shape, nd, tsc, extra)
-        more = {} if G is None else {"gforce": G}
+        F, out, S, more = run_case(name, seed, shape, nd, tsc, extra)
         np.savez_compressed(os.path.join(here, f"{name}.npz"), inp=np.stack(F), out=np.stack(out), nd=nd,
                             shape=np.array(shape), dt=tsc["dt"], at=tsc["at"], dat=tsc["dat"], ath=tsc["ath"],
                             dmax=extra.get("dmax", 2e10), **more)

@@ -1,5 +1,7 @@
 """Pin the C oracle against the golden vectors of the independent Python
-restatement (tests/golden/gen_golden.py): one sweep per case, bit-exact."""
+restatement (tests/golden/gen_golden.py): one sweep per case, bit-exact --
+the STENCIL sweep, and the non-STENCIL build's full-pencil solver for the
+pencil_* cases."""
 import glob
 import os
 
@@ -38,16 +40,32 @@ def oracle_scalars(oracle, z):
 @pytest.mark.parametrize("name", golden_cases())
 def test_oracle_matches_golden(oracle, name):
     z, inp, out = load_case(name)
-    st = oracle.OracleState(*inp, gforce=z["gforce"] if "gforce" in z.files else None)
+    st = oracle.OracleState(*inp, gforce=z["gforce"] if "gforce" in z.files else None,
+                            cho=z["cho"] if "cho" in z.files else None)
     s = oracle_scalars(oracle, z)
-    assert st.ppmsolver(s, int(z["nd"])) == 0
+    if name.startswith("pencil"):  # the non-STENCIL build's full-pencil solver
+        assert st.ppmsolver_pencil(s, int(z["nd"])) == 0
+    else:
+        assert st.ppmsolver(s, int(z["nd"])) == 0
     for q in range(5):
         a, b = st.f[q], out[q]
         assert np.array_equal(a, b), (name, q, np.abs(a - b).max())
 
 
 def test_golden_set_present():
-    assert len(GOLDEN) >= 9, "run tests/golden/gen_golden.py"
+    assert len(GOLDEN) >= 13, "run tests/golden/gen_golden.py"
+
+
+def test_pencil_peak_case_exercises_the_peaks():
+    """pencil_peak_x must reach the full-pencil solver's density-peak paths:
+    a cell above dmax x both x neighbours (pmean with cho3d) and a face
+    window with rho(2) > dmax rho(1), rho(3) > dmax rho(4) (the fix)."""
+    z, inp, _ = load_case("pencil_peak_x")
+    r, dmax, cho = inp[1], float(z["dmax"]), z["cho"]
+    cell = (r[1:-1] > dmax * r[:-2]) & (r[1:-1] > dmax * r[2:])
+    assert cell.any() and np.isin(cho[1:-1][cell], (1.0, 2.0)).any()
+    face = (r[1:-2] > dmax * r[:-3]) & (r[2:-1] > dmax * r[3:])
+    assert face.any()
 
 
 def test_gravity_cases_have_a_source():
