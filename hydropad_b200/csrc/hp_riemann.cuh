@@ -514,9 +514,24 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
     if (pattern == 1 || pattern == 2) {
         double cleft = 0.0, cright = 0.0;
         if (pattern == 2) {
-            cleft = sqrt(k.gamma * L.p / L.rho);
-            cright = sqrt(k.gamma * R.p / R.rho);
-            pm = start_shock_rarefaction<Pow>(L, R, cleft, cright, k);
+            if constexpr (Pow::kShortNewton) {
+                // mixed path: its start value and its FP32 sampling take the
+                // Eulerian sound speeds in FP32 (mixed_newton_start forms the
+                // same values); the FP64 ones only when that start fails
+                pm = mixed_newton_start(L.p, R.p, L.rho, R.rho, L.u, R.u, k);
+                const float g = float(k.gamma);
+                cleft = double(sqrtf(g * float(L.p) / float(L.rho)));
+                cright = double(sqrtf(g * float(R.p) / float(R.rho)));
+                if (!(pm > 0.0)) {
+                    cleft = sqrt(k.gamma * L.p / L.rho);
+                    cright = sqrt(k.gamma * R.p / R.rho);
+                    pm = start_shock_rarefaction<Pow>(L, R, cleft, cright, k);
+                }
+            } else {
+                cleft = sqrt(k.gamma * L.p / L.rho);
+                cright = sqrt(k.gamma * R.p / R.rho);
+                pm = start_shock_rarefaction<Pow>(L, R, cleft, cright, k);
+            }
         } else {
             pm = start_two_shocks<Pow>(L, R, k);
         }
