@@ -25,10 +25,12 @@
 //          tracing -> left state of face e-2 (ls ring), right state of
 //          face e-3 (registers)
 //   C      face e-3: Riemann problem                     -> face ring
-//   D      cell e-4: update from faces e-4 and e-3, store
+//   D      cell e-4: update from faces e-4 and e-3, store (the full-pencil
+//          solver of the non-STENCIL build: the new total energy of cell
+//          e-4, then the update of cell e-5)
 //
 // Periodicity is a wrap of the pencil index: the walk starts at cell -4
-// (= N-4) and ends at N+3; the original values of cells 0..2, which the
+// (= N-4) and ends at N+3 (N+4); the original values of cells 0..2, which the
 // walk re-reads at its end after they have been updated, are kept in a
 // small save area.
 //
