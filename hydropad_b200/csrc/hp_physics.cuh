@@ -266,50 +266,6 @@ __device__ __forceinline__ void integrate(const FaceState& f1, const FaceState& 
     w = vznew;
 }
 
-// The mixed path's update: integrate() with FP64 multiply-adds (each fused
-// operation rounds once), the factor (dt/ath)/dx formed once and the mass
-// flux of a face reused by its momentum fluxes; the same quantities as
-// integrate() to an ulp or two.  STENCIL dual energy (ee2 = etotnew).
-template <bool GRAV, class Div>
-__device__ __forceinline__ void integrate_fma(const FaceState& f1, const FaceState& f2, double& pres, double& rho,
-                                              double& u, double& v, double& w, double etot, double eint,
-                                              const Consts& k, const StepScalars& s, double ghalf) {
-    const double gamma = k.gamma, rgamma1 = k.rgamma1;
-    const double c = s.rdtath * k.rdx;
-    const double m1 = f1.rho * f1.u, m2 = f2.rho * f2.u;  // mass fluxes
-    double rhonew = fma(c, m1 - m2, rho);
-    double mx = fma(c, fma(m1, f1.u, f1.p) - fma(m2, f2.u, f2.p), u * rho);
-    if constexpr (GRAV) mx = fma(s.rdtath, (rho + rhonew) * ghalf * 0.5, mx);
-    const double vxnew = Div::div(mx, rhonew);
-    const double vynew = Div::div(fma(c, m1 * f1.v - m2 * f2.v, rho * v), rhonew);
-    const double vznew = Div::div(fma(c, m1 * f1.w - m2 * f2.w, rho * w), rhonew);
-    const double gr = gamma * rgamma1;
-    const double ke1 = fma(f1.u, f1.u, fma(f1.v, f1.v, f1.w * f1.w));
-    const double ke2 = fma(f2.u, f2.u, fma(f2.v, f2.v, f2.w * f2.w));
-    const double e1 = fma(0.5 * f1.rho, ke1, gr * f1.p) * f1.u;
-    const double e2 = fma(0.5 * f2.rho, ke2, gr * f2.p) * f2.u;
-    double etotnew = fma(c, e1 - e2, etot);
-    if constexpr (GRAV) etotnew = fma(s.rdtath, (rho * u + rhonew * vxnew) * ghalf * 0.5, etotnew);
-    const double pmean = (f1.p + f2.p) * 0.5;
-    double eintnew = fma(c * pmean, f1.u - f2.u, eint);
-    eintnew = fma(c * rgamma1, f1.p * f1.u - f2.p * f2.u, eintnew);
-    if (eintnew < 0.0) eintnew = eint;
-    const double vvv = fma(vxnew, vxnew, fma(vynew, vynew, vznew * vznew));
-    const double eeaux = fma(-0.5 * rhonew, vvv, etotnew);
-    const double ee = Div::div(eeaux, etotnew);  // ee1 and ee0 of integrate.F90:89-92
-    if (ee >= k.eta2) eintnew = eeaux;
-    double pnew;
-    if (ee >= k.eta1) pnew = (gamma - 1.0) * eeaux;
-    else pnew = (gamma - 1.0) * eintnew;
-    if (eintnew <= 0.0) pnew = pres;
-    if (rhonew <= 0.0) rhonew = rho;
-    pres = pnew;
-    rho = rhonew;
-    u = vxnew;
-    v = vynew;
-    w = vznew;
-}
-
 // New total energy of a cell from its two faces, ppm.F90:563-567 with the
 // gravity term zero (ghalf = 0, :93): the update's and the neighbours' value.
 __device__ __forceinline__ double etot_new(const FaceState& f1, const FaceState& f2, double etot, const Consts& k,

@@ -77,7 +77,6 @@ struct PolicyFP64 {
     using RareT = double;      // closed two-rarefaction form
     using PowRare = PowRoot;
     using DivD = DivIEEE;      // divisions of the update
-    static constexpr bool kFmaUpdate = false;  // the reference's operations in the update
 };
 // Mixed precision: reconstruction, flattening, characteristic tracing and
 // the traced face states in FP32; the Riemann solver's Newton for p*, u*,
@@ -91,7 +90,6 @@ struct PolicyMixed {
     using RareT = float;         // closed two-rarefaction form: no iteration
     using PowRare = PowRareF32;
     using DivD = PowRootShort;   // update divisions from a refined reciprocal (an ulp or two)
-    static constexpr bool kFmaUpdate = true;   // FP64 multiply-adds in the update
 };
 
 template <int AXIS>
@@ -686,22 +684,15 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 load_faces(d, f1, f2);
                 double p, rho, u, v, w;
                 cell_state(d, g, p, rho, u, v, w);
+                // total() with the natural component order (ppmsolver.F90:149,277,405)
+                double etot;
+                if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
+                else etot = total_energy(p, rho, u, v, w, k.rgamma1);
                 const double eint = p * k.rgamma1;
-                if constexpr (Policy::kFmaUpdate) {
-                    const double etot = fma(0.5 * rho, fma(u, u, fma(v, v, w * w)), eint);
-                    double ghalf = 0.0;
-                    if constexpr (GRAV) ghalf = S.sg[L::idx(d, tp)];
-                    integrate_fma<GRAV, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, ghalf);
+                if constexpr (GRAV) {
+                    integrate<true, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[L::idx(d, tp)]);
                 } else {
-                    // total() with the natural component order (ppmsolver.F90:149,277,405)
-                    double etot;
-                    if (AXIS == 2) etot = total_energy(p, rho, w, v, u, k.rgamma1);
-                    else etot = total_energy(p, rho, u, v, w, k.rgamma1);
-                    if constexpr (GRAV) {
-                        integrate<true, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, S.sg[L::idx(d, tp)]);
-                    } else {
-                        integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
-                    }
+                    integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
                 }
                 finish_cell(g, p, rho, u, v, w);
             }
