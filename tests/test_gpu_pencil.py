@@ -73,14 +73,15 @@ def test_pencil_differs_from_stencil(oracle):
     assert rel_l1(interior(outs[0][0]), interior(outs[1][0])) > 1e-8
 
 
-@pytest.mark.parametrize("case,n,steps,cour", [("sod", 32, 10, 0.8), ("grf", 24, 10, 0.8),
-                                               ("grf_static", 12, 4, 0.8)])
-def test_evolve_pencil(oracle, case, n, steps, cour):
+@pytest.mark.parametrize("case,n,steps,cour,zero_old", [("sod", 32, 10, 0.8, False), ("grf", 24, 10, 0.8, False),
+                                                        ("grf", 24, 10, 0.8, True), ("grf_static", 12, 4, 0.8, False)])
+def test_evolve_pencil(oracle, case, n, steps, cour, zero_old):
     """The static GRF box at Courant number 0.8 also runs the density
     fallback of the solver's update (ppm.F90:651) in a few cells, which the
     solver's characteristic speeds (the next cell's sound speed) reach
-    there."""
-    state, prm = _case(oracle, case, n, cour=cour)
+    there.  zero_old: expand with the non-STENCIL build's vxold / pold3d,
+    allocated as zeros and never assigned (alloc_arrays.F90:132-133)."""
+    state, prm = _case(oracle, case, n, cour=cour, expand_zero_old=zero_old)
     st = oracle.OracleState(*state)
     s = oracle.make_scalars(prm)
     s.pencil = 1
