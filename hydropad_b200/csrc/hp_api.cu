@@ -97,11 +97,16 @@ int copy_ctl_to_host(hp_ctx* x) {
 // interior); a kernel extracts the interior on the way in and writes the
 // interior plus its periodic ghost layers on the way out, so the host
 // array comes back with its ghosts filled (exchange_mesh.F90:23-41 for one
-// rank).  All on the context's stream.
-constexpr size_t kStageBytes = size_t(32) << 20;
+// rank).  All on the context's stream, so each chunk's copy waits for the
+// previous chunk's kernel: the stage holds a whole ghosted field up to
+// 256 MB (a 256^3 field in one chunk), which keeps those gaps to a few per
+// field.
+constexpr size_t kStageBytes = size_t(256) << 20;
 
-int ensure_stage(hp_ctx* x, size_t plane_bytes) {
+int ensure_stage(hp_ctx* x, size_t plane_bytes, int nzg) {
+    const size_t field = plane_bytes * (size_t)nzg;  // the whole ghosted field
     size_t want = plane_bytes > kStageBytes ? plane_bytes : (kStageBytes / plane_bytes) * plane_bytes;
+    if (want > field) want = field;
     if (x->stage && x->stage_bytes >= want) return HP_OK;
     HP_CUDA(cudaStreamSynchronize(x->stream));
     cudaFree(x->stage);
@@ -118,7 +123,7 @@ int upload_field(hp_ctx* x, const double* host, double* f, int nb) {
         return cuda_fail(cudaMemcpyAsync(f, host, (size_t)nx * ny * nz * sizeof(double), cudaMemcpyHostToDevice,
                                          x->stream));
     const size_t plane = (size_t)(nx + 2 * nb) * (ny + 2 * nb);
-    int rc = ensure_stage(x, plane * sizeof(double));
+    int rc = ensure_stage(x, plane * sizeof(double), nz + 2 * nb);
     if (rc != HP_OK) return rc;
     const int per = (int)(x->stage_bytes / (plane * sizeof(double)));
     for (int zg = nb; zg < nb + nz; zg += per) {
@@ -138,7 +143,7 @@ int download_field(hp_ctx* x, const double* f, double* host, int nb) {
                                          x->stream));
     const int nzg = nz + 2 * nb;
     const size_t plane = (size_t)(nx + 2 * nb) * (ny + 2 * nb);
-    int rc = ensure_stage(x, plane * sizeof(double));
+    int rc = ensure_stage(x, plane * sizeof(double), nzg);
     if (rc != HP_OK) return rc;
     const int per = (int)(x->stage_bytes / (plane * sizeof(double)));
     for (int zg = 0; zg < nzg; zg += per) {
