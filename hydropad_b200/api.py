@@ -142,11 +142,20 @@ class Hydro:
         L.check(L.lib().hp_sync_to_host(self._ctx), "hp_sync_to_host")
         return self._host
 
-    def download(self, nbound: int | None = None):
-        """Return (p, rho, vx, vy, vz) as new ghosted Fortran arrays."""
+    def download(self, nbound: int | None = None, out=None):
+        """Return (p, rho, vx, vy, vz) as ghosted Fortran arrays: new ones, or
+        the five arrays of ``out`` (float64, Fortran order, the ghosted shape),
+        e.g. views of pinned host memory, which the copies reach at full
+        speed."""
         nb = self.params.nbound if nbound is None else nbound
         shp = tuple(int(n) + 2 * nb for n in self.params.shape)
-        out = [np.zeros(shp, dtype=np.float64, order="F") for _ in range(5)]
+        if out is None:
+            out = [np.zeros(shp, dtype=np.float64, order="F") for _ in range(5)]
+        else:
+            out = list(out)
+            if len(out) != 5 or any(a.shape != shp or a.dtype != np.float64 or not a.flags.f_contiguous
+                                    for a in out):
+                raise ValueError(f"download: out must be five float64 Fortran-ordered arrays of shape {shp}")
         L.check(L.lib().hp_download_state(self._ctx, *[_dptr(a) for a in out], *shp, nb), "hp_download_state")
         return out
 

@@ -329,7 +329,9 @@ class GpuEngine:
         self.batch.remove(h)
 
     def finish(self, h):
-        return h.download(nbound=0) if self.download else None
+        if not self.download:
+            return None
+        return h.download(nbound=0, out=pinned_fields(tuple(int(n) for n in h.params.shape)))
 
     def release(self, h):
         side = int(h.params.shape[0])
@@ -364,16 +366,31 @@ def tune_tiles(precision: str, sides=(64, 128, 192, 256), device: int = 0):
     return tuple(tiles)
 
 
+def pinned_fields(shape):
+    """Five float64 Fortran-ordered arrays of ``shape`` in pinned host memory
+    (torch's caching host allocator: a block freed with its arrays is handed
+    out again), so that a finished box's download runs at DMA speed instead
+    of faulting in fresh pageable pages."""
+    import torch
+    n = int(np.prod(shape))
+    return [torch.empty(n, dtype=torch.float64, pin_memory=True).numpy().reshape(shape, order="F")
+            for _ in range(5)]
+
+
 def warm_up(sides=range(32, 257, 16), device: int = 0):
     """Server start-up: one initial-condition draw per admissible side, so
     that the FFT plans and kernels of the generator exist before the first
-    request (the first draw of a side in a process costs tens of ms)."""
+    request (the first draw of a side in a process costs tens of ms), and
+    the pinned result buffers of each side, so that no request pays for
+    pinning host memory."""
     import torch
 
     from . import ics
     for side in sides:
         ics.grf_eds_device(int(side), seed=0, device=f"cuda:{device}", noise="device")
     torch.cuda.synchronize(device)
+    for side in sorted({int(s) for s in sides}, reverse=True):
+        pinned_fields((side, side, side))  # allocated and freed: left in the cache
 
 
 def run_alone(req: Request, precision: str, tiles=None, device: int = 0):

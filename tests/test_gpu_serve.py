@@ -58,3 +58,29 @@ def test_attach_device_state_roundtrip():
         out = h.download(nbound=0)
     for a, d in zip(out, dev):
         assert np.array_equal(a, d.cpu().numpy().transpose(2, 1, 0))
+
+
+def test_download_into_pinned_buffers():
+    """The serving engine reads finished boxes back into pinned host arrays
+    (download(out=...)): the same bits as a download into new arrays, with
+    and without ghosts; arrays of another shape or order are refused."""
+    from hydropad_b200 import ics
+    from hydropad_b200.api import Hydro
+    from hydropad_b200.params import HydroParams
+    from hydropad_b200.serve import pinned_fields
+    n = 20
+    with Hydro(HydroParams(shape=(n, n, n), cosmo=True), precision="mixed") as h:
+        h.attach_device(*ics.grf_eds_device(n, seed=6, device="cuda"))
+        h.start_with_cfl()
+        h.evolve(2)
+        for nb in (0, 3):
+            ref = h.download(nbound=nb)
+            bufs = pinned_fields((n + 2 * nb,) * 3)
+            out = h.download(nbound=nb, out=bufs)
+            assert all(o is b for o, b in zip(out, bufs))
+            for a, b in zip(out, ref):
+                assert np.array_equal(a, b)
+        with pytest.raises(ValueError):
+            h.download(nbound=0, out=pinned_fields((n, n, n + 1)))
+        with pytest.raises(ValueError):
+            h.download(nbound=0, out=[np.zeros((n, n, n)) for _ in range(5)])  # C order
