@@ -9,14 +9,23 @@ cell, that state reads see original (pre-sweep) values, that no phase reads
 what another thread writes in the same phase, and that every cell is written
 exactly once.  It covers all pencil lengths the kernel accepts for the tile
 shapes it is compiled with.
+
+lag=1 replays the non-STENCIL build's full-pencil solver (PENCIL): the walk
+runs one cell further, the density-peak window of face f is cells
+f-2..f+1, and stage D splits in two: D1 writes the new total energy of
+cell e-4 to a ring, D2 (after a barrier) updates cell e-5 from its faces,
+its state, its old neighbours' densities and the new total energies of
+cells e-6..e-4 (0 beyond the pencil's ends).
 """
 import pytest
 
-# (T, RING) of the compiled tiles: x sweep and y/z sweeps
-TILES = [(32, 64), (8, 16), (16, 32)]
+from tests.test_sweep_layout import tile_table
+
+# (T, RING) of the compiled tiles, every axis
+TILES = sorted({(T, ring) for _axis, _tile, _P, T, ring, _minb in tile_table()})
 
 
-def emulate(N, T, R):
+def emulate(N, T, R, lag=0):
     glob = {c: ("orig", c) for c in range(N)}
     written = {}
     ring = {}
@@ -25,19 +34,19 @@ def emulate(N, T, R):
     FS = {}
     save = {}
     right = {}
-
+    SE = {}
 
     def wrap(c):
         return c % N
 
     b = -4
-    while b <= N + 3:
+    while b <= N + 3 + lag:
         es = [b + tl for tl in range(T)]
         # ---- load ----
         reads_save, writes = set(), {}
         for tl, e in enumerate(es):
             if -4 <= e <= N + 2:
-                from_save = e >= N and (e + 4) // T > (e - N + 8) // T
+                from_save = e >= N and (e + 4) // T > (e - N + 8 + lag) // T
                 if from_save:
                     reads_save.add(e - N)
                     val = save[e - N]
@@ -90,18 +99,33 @@ def emulate(N, T, R):
         for f in work:
             assert LS[(f - 1) % R] == f - 1
             assert FS[f % R] == ("right", f)
-            for x in range(f - 3, f + 1):
+            for x in range(f - 3, f + 1 + lag):  # the peak window (f-2..f+1 with lag)
                 state_ok(x)
             wr[f % R] = ("face", f)
         FS.update(wr)
-        # ---- D ----
+        # ---- D (lag: D1, barrier, D2) ----
         wr = {}
+        if lag:
+            wse = {}
+            for e in es:
+                d = e - 4
+                if 0 <= d < N:
+                    assert FS[d % R] == ("face", d) and FS[(d + 1) % R] == ("face", d + 1)
+                    state_ok(d)
+                    wse[d % R] = ("etot", d)
+            SE.update(wse)
         for tl, e in enumerate(es):
-            d = e - 4
+            d = e - 4 - lag
             if 0 <= d < N:
                 assert FS[d % R] == ("face", d), (N, T, d, FS[d % R])
                 assert FS[(d + 1) % R] == ("face", d + 1)
                 state_ok(d)
+                if lag:
+                    for x in (d - 1, d + 1):
+                        state_ok(x)  # the old neighbours of the peak test
+                    for x in (d - 1, d, d + 1):
+                        if 0 <= x < N:
+                            assert SE[x % R] == ("etot", x), (N, T, d, x, SE.get(x % R))
                 wr[d] = ("new", d)
         for d, v in wr.items():
             assert d not in written
@@ -111,13 +135,19 @@ def emulate(N, T, R):
     assert sorted(written) == list(range(N))
 
 
+def test_tiles_read():
+    assert len(TILES) >= 5
+
+
+@pytest.mark.parametrize("lag", [0, 1])
 @pytest.mark.parametrize("T,R", TILES)
-def test_schedule_all_lengths(T, R):
+def test_schedule_all_lengths(T, R, lag):
     for N in range(8, 200):
-        emulate(N, T, R)
+        emulate(N, T, R, lag)
 
 
-def test_schedule_large_pencils():
+@pytest.mark.parametrize("lag", [0, 1])
+def test_schedule_large_pencils(lag):
     for T, R in TILES:
         for N in (256, 511, 512, 1024):
-            emulate(N, T, R)
+            emulate(N, T, R, lag)
