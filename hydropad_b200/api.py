@@ -7,9 +7,9 @@ follow the reference routines they replace:
 ``ppmsolver(nd)``      hydro/ppmsolver.F90:1-467 (one directional sweep)
 ``ppm_lxlylz(nrot)``   hydro/ppm_lxlylz.F90:1-223 (+ exchange_mesh)
 ``speed()``            hydropad/speed.F90:2-59
-``timedet(velmax)``    hydropad/functions.F90:61-210
+``timedet(velmax)``    hydropad/functions.F90:2-151
 ``evolve(nsteps)``     hydro part of evolve_sys.F90:30-130, looped as in
-                       main.F90:200-221
+                       main.F90:100-121
 ``attach_state``       the `!$acc update device` of ppmsolver.F90:95
 ``sync_to_host``       the `!$acc update host` of ppm_lxlylz.F90:20
 =====================  =====================================================

@@ -7,7 +7,7 @@ queue) and runs timedet once per member; every member follows its own
 evolve_sys step exactly (its own nrot, dt, nstep), so a box advanced in a
 batch is bitwise identical to the same box advanced alone with the same
 tiles.  The reference has no counterpart: it advances one box per run
-(hydropad/main.F90:200-221).
+(hydropad/main.F90:100-121).
 """
 from __future__ import annotations
 

@@ -21,7 +21,7 @@ enum : int {
     kFlagExpand = 2,       // apply expand.F90 to the updated cells
     kFlagSpeed = 4,        // accumulate velmax of the updated cells
     kFlagResetSpeed = 8,   // zero the velmax accumulator (first sweep of a step)
-    kFlagExpandZeroOld = 16,  // expand with vxold = pold3d = 0 (as alloc_arrays.F90:178-181 leaves them)
+    kFlagExpandZeroOld = 16,  // expand with vxold = pold3d = 0 (as alloc_arrays.F90:71-74,132-135 leaves them)
     kFlagZHalo = 32,       // z sweep of a slab: the cells beyond its ends come from halo planes
 };
 

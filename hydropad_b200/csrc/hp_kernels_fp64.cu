@@ -56,6 +56,8 @@ int launch_bounds(const Box& b, int slot, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // speed.F90:17-31: velmax over the resident state (accumulator zeroed first).
+// (The sweep's epilogue computes the same maximum for hp_evolve; this kernel
+// serves hp_speed.)
 // ---------------------------------------------------------------------------
 __global__ void speed_kernel(const double* __restrict__ p, const double* __restrict__ rho,
                              const double* __restrict__ vx, const double* __restrict__ vy,
@@ -81,12 +83,12 @@ int launch_speed(const Box& b, cudaStream_t st) {
 }
 
 // ---------------------------------------------------------------------------
-// timedet (functions.F90:61-94) / timedet_cosmo (functions.F90:97-210, EdS)
+// timedet (functions.F90:2-35) / timedet_cosmo (functions.F90:38-151, EdS)
 // on the device control block, with velmax from the accumulator.  Advances
 // the step counter (when `advance`: the end of an evolve_sys step) and
-// raises `done` when told reaches tstop (main.F90:200).
+// raises `done` when told reaches tstop (main.F90:100).
 // ---------------------------------------------------------------------------
-constexpr double kC0P1 = 0.10000000149011612;   // 0.1 (functions.F90:80,155)
+constexpr double kC0P1 = 0.10000000149011612;   // 0.1 (functions.F90:21,96)
 constexpr double kTwo3 = 0.6666666865348816;    // 2.0/3.0 as REAL(4)
 constexpr double kMThird = -0.3333333432674408; // -1.0/3.0 as REAL(4)
 

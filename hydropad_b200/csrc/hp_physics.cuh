@@ -13,13 +13,13 @@
 namespace hp {
 
 // REAL(4) literals of the reference, promoted to REAL(8).
-constexpr double kSixth = 0.1666666716337204;      // 0.16666667  ppm_functs.F90:33-34, dda.F90:198-199
+constexpr double kSixth = 0.1666666716337204;      // 0.16666667  ppm_functs.F90:33-34, dda.F90:17-18
 constexpr double kThird = 0.3333333432674408;      // 0.33333333  ppm_functs.F90:103,122
 constexpr double kTiny = 1.0000000036274937e-15;   // 1e-15       order2interp.F90:176-189
-constexpr double kTerr = 0.0010000000474974513;    // 1e-3        riemann.F90:337
-constexpr double kC010 = 0.009999999776482582;     // 0.010       dda.F90:200
-constexpr double kC050 = 0.05000000074505806;      // 0.050       dda.F90:203
-constexpr int kNewtonMax = 100;                     // riemann.F90:339
+constexpr double kTerr = 0.0010000000474974513;    // 1e-3        riemann.F90:48
+constexpr double kC010 = 0.009999999776482582;     // 0.010       dda.F90:19
+constexpr double kC050 = 0.05000000074505806;      // 0.050       dda.F90:22
+constexpr int kNewtonMax = 100;                     // riemann.F90:50
 
 // Fortran MIN/MAX of two reals (first operand kept on ties and NaN in b).
 template <class R> __device__ __forceinline__ R fmin2(R a, R b) { return b < a ? b : a; }
@@ -66,7 +66,7 @@ __device__ __forceinline__ bool flat_pair(R left, R right, R mingradflat) {
     }
 }
 
-// Second difference used by dda (dda.F90:198-199), centred on the middle cell.
+// Second difference used by dda (dda.F90:17-18), centred on the middle cell.
 template <class R>
 __device__ __forceinline__ R dda_second(R am1, R a, R ap1, R dx) {
     return R(kSixth) * (ap1 - R(2) * a + am1) / (dx * dx);
@@ -80,7 +80,7 @@ struct Parabola {
 
 // correction() without the tracing part: q0..q4 are cells c-2..c+2, dm,d0,dp
 // the ajside slopes of c-1,c,c+1.  For rho with addrho >= addp the contact
-// steepening of dda() blends in (dda.F90:196-214, ppm_functs.F90:35-40);
+// steepening of dda() blends in (dda.F90:15-33, ppm_functs.F90:35-40);
 // Dm,Dp are the second differences centred on c-1 and c+1.
 template <class R>
 __device__ __forceinline__ Parabola<R> build_parabola(R q1, R q2, R q3, R dm, R d0, R dp, R flat,

@@ -14,17 +14,17 @@
 namespace hp {
 
 template <class S = double>
-__device__ __forceinline__ S rarwave(S f1, S f2, S vt, S vh) {  // :290-298
+__device__ __forceinline__ S rarwave(S f1, S f2, S vt, S vh) {  // riemann.F90:1-9
     return f2 + vt * (f1 - f2) / (vt - vh);
 }
 template <class S = double>
-__device__ __forceinline__ S rhoshock(S p2, S p1, S rho1, S gamma1) {  // :303-313
+__device__ __forceinline__ S rhoshock(S p2, S p1, S rho1, S gamma1) {  // riemann.F90:14-24
     return rho1 * (gamma1 * p2 / p1 + S(1)) / (gamma1 + p2 / p1);
 }
 
 // ------------------------------------------------------------------------
 // Powers by exponent: x^m, x^-gf, x^rgamma, x^rm
-// (riemannsolver.F90:63,118-119,126,158,192-199; riemann.F90:360-385).
+// (riemannsolver.F90:63,118-119,126,158,192-199; riemann.F90:71-96).
 // ------------------------------------------------------------------------
 
 // CUDA pow, out of line so that all call sites share one copy of its code.
@@ -185,7 +185,7 @@ struct PowF32m {
 };
 
 // ------------------------------------------------------------------------
-// riemann, riemann.F90:318-400 (van Leer Newton for p*).  Returns false when
+// riemann, riemann.F90:29-111 (van Leer Newton for p*).  Returns false when
 // more than 100 iterations would be needed (the reference stops the run).
 // ------------------------------------------------------------------------
 // Start value of the mixed path's Newton iteration: the two-rarefaction
@@ -195,7 +195,7 @@ struct PowF32m {
 // number, the linearised (acoustic) estimate (pL+pR)/2 + kappa (uL-uR)/2;
 // 0 if neither is positive.
 //
-// The reference's guess (riemann.F90:343-345) adds kappa (uL+uR)/2, which in
+// The reference's guess (riemann.F90:54-56) adds kappa (uL+uR)/2, which in
 // the bulk flows of a cosmological box lands far from the root: on a 48^3
 // EdS field its Newton faces take 4.9 iterations on average and 7.9 for the
 // slowest face of 32 (a warp waits for its slowest lane), the linearised
@@ -223,7 +223,7 @@ __device__ __forceinline__ double mixed_newton_start(double pleft, double pright
     return pcheck > 0.0 ? pcheck : 0.0;
 }
 
-// riemann.F90:318-400 with the divisions of the loop body replaced by
+// riemann.F90:60-109 with the divisions of the loop body replaced by
 // products with reciprocals formed once (or by rsqrt), and u* formed once
 // after the loop from the last wave speeds: the same iterates up to a few
 // ulp, with a shorter dependency chain per iteration.  Both paths run it in
@@ -303,7 +303,7 @@ __device__ __forceinline__ bool riemann_newton(double& pstar, double& vstar, dou
                                                double rholeft, double rhoright, double vxleft, double vxright,
                                                const Consts& k) {
     if constexpr (!Pow::kShortNewton) {
-        // the reference's start value (riemann.F90:343-345)
+        // the reference's start value (riemann.F90:54-56)
         const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
         const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft + vxright);
         if (pcheck > 0.0) pstar = pcheck;

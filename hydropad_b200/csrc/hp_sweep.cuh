@@ -214,7 +214,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     const StepScalars sc = a.ctl->s;
     const R dt_ = R(sc.dt), rat_ = R(sc.rat), dat_ = R(sc.dat), at_ = R(sc.at);
     const R dx_ = R(k.dx), gam_ = R(k.gamma), flatv_ = R(k.flatvalue), ming_ = R(k.mingradflat);
-    if (a.ctl->done) return;  // told >= tstop: the time loop has ended (main.F90:200)
+    if (a.ctl->done) return;  // told >= tstop: the time loop has ended (main.F90:100)
 
     // density-peak fix is possible only if some rho exceeds dmax x another
     // rho (monotone rounding makes this test exact; see the update epilogue)
@@ -229,7 +229,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         if (a.flags & kFlagResetSpeed) a.ctl->velmax_key = 0ULL;
     }
 
-    // expand.F90:157-159
+    // expand.F90:18-20
     const double afact = sc.dt * (sc.dath / sc.ath);
     const double afact1 = 1.0 / (1.0 + afact);
     const double afact2 = 1.0 / (2.0 + afact);
@@ -287,7 +287,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     // D's epilogue: expand, store, and the step's reductions
     auto finish_cell = [&](long long g, double p, double rho, double u, double v, double w) {
         if (a.flags & kFlagExpand) {
-            // expand.F90:161-176 with the step-start snapshot
+            // expand.F90:22-41 with the step-start snapshot
             const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
             const double vx_o = zero_old ? 0.0 : a.snap[1][g];
             const double vy_o = zero_old ? 0.0 : a.snap[2][g];

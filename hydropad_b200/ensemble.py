@@ -8,7 +8,7 @@ seed per box (all from ``--seed``), started together at a = 1/51 and
 advanced ``--steps`` evolve_sys steps each.  The batch is autotuned, then
 timed with CUDA events on its stream; ``--alone`` also times the same boxes
 advanced one after another through hp_evolve (the one-box-per-run layout of
-the reference's main program, hydropad/main.F90:200-221).  Prints one JSON
+the reference's main program, hydropad/main.F90:100-121).  Prints one JSON
 line (aggregate cell-updates/s).
 
 Under torchrun (one process per GPU) the boxes are split across the ranks by

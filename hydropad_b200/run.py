@@ -3,7 +3,7 @@
     python -m hydropad_b200.run --case eds --n 256 --steps 10 --precision mixed
     python -m hydropad_b200.run --case sod --n 64 --steps 100 --precision fp64 --tiles 4,4,4
 
-Mirrors the reference's main program for the hydro part (main.F90:200-221:
+Mirrors the reference's main program for the hydro part (main.F90:100-121:
 the time loop over evolve_sys) on synthetic initial conditions, and prints
 one JSON line with the step count, simulated time, wall time and
 cell-updates/s.  Used for profiling single configurations.

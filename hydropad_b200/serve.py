@@ -19,7 +19,7 @@ box's final state, downloaded to the host.  The server keeps one
 
 Every member follows its own evolve_sys step, so a response is bitwise the
 result of the same request run alone.  The reference has no serving layer:
-it advances one box per run (hydropad/main.F90:200-221).
+it advances one box per run (hydropad/main.F90:100-121).
 
 The scheduling logic (:class:`Scheduler`) is independent of the GPU: it
 drives an engine object, which :class:`GpuEngine` implements on the library

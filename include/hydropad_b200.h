@@ -12,9 +12,9 @@
  *                      hydropad/exchange_mesh.F90:23-41)
  *   hp_speed       <- SUBROUTINE speed               hydropad/speed.F90:2-59
  *   hp_timedet     <- SUBROUTINE timedet / timedet_cosmo
- *                                                    hydropad/functions.F90:61-210
+ *                                                    hydropad/functions.F90:2-151
  *   hp_evolve      <- the hydro part of SUBROUTINE evolve_sys, nsteps times
- *                     hydropad/evolve_sys.F90:30-130, main.F90:200-221
+ *                     hydropad/evolve_sys.F90:30-130, main.F90:100-121
  *   hp_attach_state / hp_sync_to_host
  *                  <- the `!$acc update device/host` pairs around every sweep
  *                     (ppmsolver.F90:95, ppm_lxlylz.F90:20), done once per run
@@ -200,7 +200,7 @@ int hp_ppmsolver_noalloc(double *p, double *rho, double *vx, double *vy,
 
 /* ---------------------------------------------------------------------
  * Batches: many independent boxes advanced together.  No counterpart in
- * the reference, which advances one box per run (main.F90:200-221, the
+ * the reference, which advances one box per run (main.F90:100-121, the
  * time loop over evolve_sys); every member box follows exactly the
  * reference's step (its own nrot, dt, nstep and tstop), so a box advanced
  * in a batch is bitwise identical to the same box advanced alone by

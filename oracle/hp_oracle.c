@@ -304,19 +304,19 @@ static void order2interp(const double *pres, const double *rho, const double *vx
 }
 
 /* ------------------------------------------------------------------ */
-/* hydro/riemannsolver.F90:290-400                                     */
+/* hydro/riemann.F90:1-111                                             */
 /* ------------------------------------------------------------------ */
-static double rarwave(double f1, double f2, double vt, double vh)   /* :290-298 */
+static double rarwave(double f1, double f2, double vt, double vh)   /* :1-9 */
 {
     return f2 + vt * (f1 - f2) / (vt - vh);
 }
 
-static double rhoshock(double p2, double p1, double rho1, const hpo_scalars *s) /* :303-313 */
+static double rhoshock(double p2, double p1, double rho1, const hpo_scalars *s) /* :14-24 */
 {
     return rho1 * (s->gamma1 * p2 / p1 + 1.0) / (s->gamma1 + p2 / p1);
 }
 
-/* riemann, :318-400.  Returns 1 on Newton non-convergence (reference: stop). */
+/* riemann, :29-111.  Returns 1 on Newton non-convergence (reference: stop). */
 static int riemann(double *pstar, double *vstar, double pleft, double pright, double rholeft,
                    double rhoright, double vxleft, double vxright, const hpo_scalars *s)
 {
@@ -1032,7 +1032,7 @@ double hpo_speed(const double *p3d, const double *rho3d, const double *vx3d, con
     return vmax;
 }
 
-/* timedet, functions.F90:61-94 */
+/* timedet, functions.F90:2-35 */
 void hpo_timedet(hpo_scalars *s)
 {
     s->at = 1.0;
@@ -1053,9 +1053,9 @@ void hpo_timedet(hpo_scalars *s)
     s->rdtath = s->dt / s->ath;
 }
 
-/* timedet_cosmo, functions.F90:97-210, omega_m == 1, COSMO defined.  The
- * particle-velocity term (:137-150) is zero without N-body.  The debug cap
- * dt0 = 1e-9 (:108,156) is applied only when s->dt_cap > 0. */
+/* timedet_cosmo, functions.F90:38-151, omega_m == 1, COSMO defined.  The
+ * particle-velocity term (:76-91) is zero without N-body.  The debug cap
+ * dt0 = 1e-9 (:49,97) is applied only when s->dt_cap > 0. */
 void hpo_timedet_cosmo(hpo_scalars *s)
 {
     double rdt, rdtc, dta;

@@ -33,7 +33,7 @@ typedef struct {
     double dx, rdx;                                   /* initialize_parameters.F90:23-24 */
     double dt, rdtath, at, dat, rat, ath, dath;       /* time scalars of the step */
     double t, told, thalf, dtold, tstop, atnew, datnew;
-    double dt_cap;   /* timedet_cosmo debug cap dt0 (functions.F90:108,156); <=0 disables */
+    double dt_cap;   /* timedet_cosmo debug cap dt0 (functions.F90:49,97); <=0 disables */
     double velmax;
     int    nstep;
     int    cosmo;    /* 1: EdS expanding background (timedet_cosmo + expand) */
@@ -81,9 +81,9 @@ double hpo_speed(const double *p3d, const double *rho3d, const double *vx3d,
                  const double *vy3d, const double *vz3d, int nx, int ny,
                  int nz, int nbound, const hpo_scalars *s);
 
-/* Static timestep (functions.F90:61-94). */
+/* Static timestep (functions.F90:2-35). */
 void hpo_timedet(hpo_scalars *s);
-/* EdS timestep (functions.F90:97-210, omega_m = 1 branch). */
+/* EdS timestep (functions.F90:38-151, omega_m = 1 branch). */
 void hpo_timedet_cosmo(hpo_scalars *s);
 /* Time initialisation (initialize_parameters.F90:133-205).  a_start is the
  * initial expansion factor (cosmo only). */
