@@ -60,10 +60,10 @@ EXPORTS = (
     "hp_batch_create", "hp_batch_destroy", "hp_batch_add", "hp_batch_remove", "hp_batch_size",
     "hp_batch_step", "hp_batch_synchronize", "hp_batch_member", "hp_batch_set_tiles", "hp_batch_get_tiles",
     "hp_batch_autotune", "hp_batch_stream", "hp_batch_launch_count",
-    "hp_set_variant", "hp_get_variant", "hp_attach_cho", "hp_ppmsolver_pencil",
+    "hp_set_variant", "hp_get_variant", "hp_attach_cho", "hp_ppmsolver_pencil", "hp_bad_cell",
 )
 _NOT_INT = ("hp_stream", "hp_strerror", "hp_launch_count", "hp_batch_member", "hp_batch_stream",
-            "hp_batch_launch_count")
+            "hp_batch_launch_count", "hp_bad_cell")
 
 _lib = None
 
@@ -115,6 +115,8 @@ def lib():
     L.hp_strerror.restype = C.c_char_p
     L.hp_launch_count.argtypes = [cp]
     L.hp_launch_count.restype = C.c_longlong
+    L.hp_bad_cell.argtypes = [cp]
+    L.hp_bad_cell.restype = C.c_longlong
     L.hp_set_tiles.argtypes = [cp, C.c_int, C.c_int, C.c_int]
     L.hp_get_tiles.argtypes = [cp, ip]
     L.hp_autotune.argtypes = [cp, C.c_int]

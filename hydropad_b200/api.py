@@ -210,9 +210,23 @@ class Hydro:
                                          C.byref(nx), C.byref(ny), C.byref(nz), C.byref(nb), C.byref(nd))
         L.check(rc, "hp_ppmsolver_pencil")
 
+    def bad_cell(self):
+        """(i, j, k) interior indices of the first cell that the last error
+        status reported (NaN, or non-positive density or pressure), or None."""
+        c = int(L.lib().hp_bad_cell(self._ctx))
+        if c < 0:
+            return None
+        nx, ny, _ = (int(v) for v in self.params.shape)
+        return (c % nx, (c // nx) % ny, c // (nx * ny))
+
+    def _check_status(self, rc: int, what: str):
+        if rc in (-5, -6):  # HP_ERR_NAN, HP_ERR_NEGATIVE_STATE: name the first cell
+            what = f"{what} (first bad cell {self.bad_cell()})"
+        L.check(rc, what)
+
     def ppm_lxlylz(self, nrot: int):
         L.check(L.lib().hp_ppm_lxlylz(self._ctx, int(nrot)), "hp_ppm_lxlylz")
-        L.check(L.lib().hp_synchronize(self._ctx), "hp_ppm_lxlylz")
+        self._check_status(L.lib().hp_synchronize(self._ctx), "hp_ppm_lxlylz")
 
     def speed(self) -> float:
         v = C.c_double()
@@ -232,7 +246,7 @@ class Hydro:
         self.timedet(self.speed())
 
     def evolve(self, nsteps: int, graph: bool = True):
-        L.check(L.lib().hp_evolve(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve")
+        self._check_status(L.lib().hp_evolve(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve")
 
     def evolve_async(self, nsteps: int, graph: bool = True):
         """Enqueue nsteps without waiting or reading the status (for timing
@@ -240,7 +254,7 @@ class Hydro:
         L.check(L.lib().hp_evolve_async(self._ctx, int(nsteps), 1 if graph else 0), "hp_evolve_async")
 
     def synchronize(self):
-        L.check(L.lib().hp_synchronize(self._ctx), "hp_synchronize")
+        self._check_status(L.lib().hp_synchronize(self._ctx), "hp_synchronize")
 
     # -- scalars ------------------------------------------------------------------
     def get_scalars(self) -> L.HpScalars:

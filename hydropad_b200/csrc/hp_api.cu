@@ -7,6 +7,7 @@
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <stddef.h>
 #include <string.h>
 
 #include <vector>
@@ -158,6 +159,8 @@ int download_field(hp_ctx* x, const double* f, double* host, int nb) {
 
 // One fused sweep on the resident state.
 int do_sweep(hp_ctx* x, int axis, int flags) {
+    static const char* const kNames[3] = {"hp sweep x", "hp sweep y", "hp sweep z"};
+    hp::TraceRange tr(kNames[axis]);
     const int bslot = (int)(x->sweep_count % 3);
     int n = 0;
     if (x->slab && axis == 2) {
@@ -290,7 +293,12 @@ int hp_init(const hp_params* p, hp_ctx** out) {
     if (p->cosmo && !p->expand_zero_old)
         for (int q = 0; q < 4; ++q)
             if ((rc = cuda_fail(cudaMalloc(&x->box.snap[q], n * sizeof(double)))) != HP_OK) return fail(rc);
-    if ((rc = cuda_fail(cudaMalloc(&x->box.peak, n * sizeof(double)))) != HP_OK) return fail(rc);
+    // density-peak values of the y/z faces: one per cell (face f < N of a
+    // pencil at its cell f) and one per pencil for the last face
+    {
+        const size_t ptail = (size_t)p->ngridx * (p->ngridy > p->ngridz ? p->ngridy : p->ngridz);
+        if ((rc = cuda_fail(cudaMalloc(&x->box.peak, (n + ptail) * sizeof(double)))) != HP_OK) return fail(rc);
+    }
     if ((rc = cuda_fail(cudaMalloc(&x->box.ctl, sizeof(hp::DevCtl)))) != HP_OK) return fail(rc);
     if ((rc = cuda_fail(cudaMallocHost(&x->ctl_pinned, sizeof(hp::DevCtl)))) != HP_OK) return fail(rc);
 
@@ -312,6 +320,7 @@ int hp_init(const hp_params* p, hp_ctx** out) {
     k.dmax = p->dmax;
     k.eta1 = p->eta1;
     k.eta2 = p->eta2;
+    k.nbound = p->nbound;
     // exponents of the Riemann solver as multiples of 1/n (see PowRoot)
     k.nroot = 0;
     k.jrg = 0;
@@ -333,6 +342,8 @@ int hp_init(const hp_params* p, hp_ctx** out) {
     c.dx = k.dx;
     c.dt_cap = p->dt_cap;
     c.nstep = 1;
+    c.bad_cell = -1;
+    x->last_bad_cell = -1;
     for (int s = 0; s < 3; ++s) {
         c.rho_key[s][0] = hp::kKeyPosInf;
         c.rho_key[s][1] = hp::kKeyNegInf;
@@ -402,6 +413,7 @@ int hp_attach_state(hp_ctx* x, const double* p3d, const double* rho3d, const dou
     if (nbound < 0 || nx != x->box.nx + 2 * nbound || ny != x->box.ny + 2 * nbound || nz != x->box.nz + 2 * nbound)
         return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(x->dev));
+    hp::TraceRange tr("hp attach state (host to device)");
     // gforce is static (initialize_gravity.F90): attaching again with the
     // same array does not upload it again
     if (!gforce) {
@@ -455,6 +467,7 @@ int hp_download_state(hp_ctx* x, double* p3d, double* rho3d, double* vx3d, doubl
     if (nbound < 0 || nx != x->box.nx + 2 * nbound || ny != x->box.ny + 2 * nbound || nz != x->box.nz + 2 * nbound)
         return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(x->dev));
+    hp::TraceRange tr("hp download state (device to host)");
     double* dst[5] = {p3d, rho3d, vx3d, vy3d, vz3d};
     for (int q = 0; q < 5; ++q) {
         const int rc = download_field(x, x->box.f[q], dst[q], nbound);
@@ -615,6 +628,7 @@ int hp_evolve_async(hp_ctx* x, int nsteps, int use_graph) {
     if (!x->attached) return HP_ERR_NOT_ATTACHED;
     HP_CUDA(cudaSetDevice(x->dev));
     for (int it = 0; it < nsteps; ++it) {
+        hp::TraceRange tr("hp step");
         const long long nstep = x->nstep_host;
         const int nrot = hp::nrot_of_step(nstep);
         const int slot = (int)(x->sweep_count % 3);
@@ -655,12 +669,22 @@ int hp_evolve(hp_ctx* x, int nsteps, int use_graph) {
 int hp_synchronize(hp_ctx* x) {
     if (!x) return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(x->dev));
-    unsigned st = 0;
-    HP_CUDA(cudaMemcpyAsync(&st, &x->box.ctl->status, sizeof st, cudaMemcpyDeviceToHost, x->stream));
-    HP_CUDA(cudaMemsetAsync(&x->box.ctl->status, 0, sizeof st, x->stream));
+    // status, done and the first bad cell are adjacent: one read
+    static_assert(offsetof(hp::DevCtl, bad_cell) == offsetof(hp::DevCtl, status) + 8, "DevCtl layout");
+    struct {
+        unsigned status;
+        int done;
+        long long bad_cell;
+    } rd;
+    HP_CUDA(cudaMemcpyAsync(&rd, &x->box.ctl->status, sizeof rd, cudaMemcpyDeviceToHost, x->stream));
+    HP_CUDA(cudaMemsetAsync(&x->box.ctl->status, 0, sizeof(unsigned), x->stream));
+    HP_CUDA(cudaMemsetAsync(&x->box.ctl->bad_cell, 0xff, sizeof(long long), x->stream));
     HP_CUDA(cudaStreamSynchronize(x->stream));
-    return hp::status_error(st);
+    if (rd.status) x->last_bad_cell = rd.bad_cell;
+    return hp::status_error(rd.status);
 }
+
+long long hp_bad_cell(hp_ctx* x) { return x ? x->last_bad_cell : -1; }
 
 void* hp_stream(hp_ctx* x) { return x ? (void*)x->stream : nullptr; }
 

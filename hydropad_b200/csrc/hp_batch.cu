@@ -324,6 +324,7 @@ int hp_batch_step(hp_batch* b, int nsteps, int use_graph) {
     std::vector<int> nrot(n);
     Plan dyn;
     for (int it = 0; it < nsteps; ++it) {
+        hp::TraceRange tr("hp batch step");
         int rc = ensure_tables(b);
         if (rc != HP_OK) return rc;
         bool aligned = true;

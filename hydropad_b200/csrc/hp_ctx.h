@@ -28,6 +28,7 @@ struct hp_ctx {
     int nz_global, z0;
     double* cho_dev;          // attached cho3d (dense) for the full-pencil solver, or null
     const double* host_cho;   // the attached host cho3d array, or null
+    long long last_bad_cell;  // first bad cell of the last non-zero status read (hp_bad_cell), or -1
 };
 
 namespace hp {

@@ -37,7 +37,16 @@ struct DevCtl {
     unsigned long long velmax_key;     // bits of a non-negative double (max accumulator)
     unsigned int status;
     int done;                          // told >= tstop: further steps are no-ops
+    // dense index of the first updated cell found with a NaN or a
+    // non-positive density or pressure since the status word was last read
+    // (-1: none); read together with `status`
+    long long bad_cell;
 };
+
+// A sweep found cell g of the box non-physical: keep the first such cell.
+__device__ __forceinline__ void record_bad_cell(DevCtl* c, long long g) {
+    atomicCAS(reinterpret_cast<unsigned long long*>(&c->bad_cell), ~0ULL, (unsigned long long)g);
+}
 
 // Order-preserving map double -> uint64 (valid for every non-NaN double).
 __device__ __forceinline__ unsigned long long dkey(double x) {

@@ -234,6 +234,7 @@ __global__ void status_gather_kernel(DevCtl* const* __restrict__ ctls, int n, un
     if (i < n) {
         out[i] = ctls[i]->status;
         ctls[i]->status = 0u;
+        ctls[i]->bad_cell = -1;
     }
 }
 
@@ -251,38 +252,76 @@ int launch_timedet(const Box& b, int advance, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Density-peak pre-pass for y/z sweeps.  The reference gathers the peak test
 // with the x-index slot in every direction (ppmsolver.F90:251-252 for y,
-// :379-380 for z): for the y face (x, y, z) it reads rho3d(y-3..y, x, z) and
-// vy3d(y-2..y-1, x, z); for the z face (x, y, z) rho3d(z-3..z, y, x) and
-// vz3d.  Those cells belong to other pencils, which the in-place sweep
-// updates concurrently, so the values are evaluated here on the pre-sweep
-// state.  Indices wrap periodically (identical to the reference's ghost
-// reads for cubic boxes).  Runs only when the rho bounds admit a peak.
+// :379-380 for z): for the y face i (between cells i-1 and i of the pencil
+// (x, z)) it reads rho3d(iaux, x, z) and vy3d(iaux, x, z), for the z face
+// rho3d(iaux, y, x) and vz3d, iaux = i-3 .. i, in its ghosted arrays
+// (nx+2nb, ny+2nb, nz+2nb), x fastest, whose ghost layers hold periodic
+// copies of the interior (exchange_mesh after every sweep).  Those cells
+// belong to other pencils, which the in-place sweep updates concurrently, so
+// the values are evaluated here on the pre-sweep state.  The gather is the
+// reference's linear index: a column index beyond the ghosted extent runs on
+// into the next row or plane (non-cubic boxes), and an index past the end
+// of the array reads nothing (NaN: the peak test is false).  Each linear
+// index is mapped back to the interior cell whose copy the reference array
+// holds there.  Runs only when the rho bounds admit a peak.
+//
+// Layout of `peak`: the value of face f < N of the pencil at the cell index
+// of its right cell f, the last face (f = N) at ncell + pencil.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void peak_prepass_box(const double* __restrict__ rho, const double* __restrict__ vn,
                                                  double* peak, int nx, int ny, int nz, int axis, double dmax,
-                                                 const DevCtl* c, int bslot, long long i0, long long di) {
+                                                 int nb, const DevCtl* c, int bslot, long long i0, long long di) {
     const double rmin0 = dkey_decode(c->rho_key[bslot][0]);
     const double rmax0 = dkey_decode(c->rho_key[bslot][1]);
     if (!(rmax0 > dmax * rmin0) || c->done) return;
     const long long n = (long long)nx * ny * nz;
-    for (long long i = i0; i < n; i += di) {
-        const int x = (int)(i % nx);
-        const int y = (int)((i / nx) % ny);
-        const int z = (int)(i / ((long long)nx * ny));
-        // (face index along the sweep, row index y', plane index z') of the
-        // x-row that the reference reads
-        int f, yy, zz;
-        if (axis == 1) { f = y; yy = x % ny; zz = z; }
-        else { f = z; yy = y; zz = x % nz; }
-        const long long row = (long long)nx * (yy + (long long)ny * zz);
-        auto at = [&](int o) { int xi = ((f + o) % nx + nx) % nx; return row + xi; };
-        peak[i] = peak_value(rho[at(-3)], rho[at(-2)], rho[at(-1)], rho[at(0)], vn[at(-2)], vn[at(-1)], dmax);
+    const long long npencil = axis == 1 ? (long long)nx * nz : (long long)nx * ny;
+    const int nsweep = axis == 1 ? ny : nz;
+    const long long gx = nx + 2 * nb, gy = ny + 2 * nb, gz = nz + 2 * nb;
+    const long long gtot = gx * gy * gz;
+    for (long long i = i0; i < n + npencil; i += di) {
+        // face f of the pencil whose transverse cell is (x, t): t = z (y sweep) or y (z sweep)
+        int x, t, f;
+        if (i < n) {
+            x = (int)(i % nx);
+            const int y = (int)((i / nx) % ny);
+            const int z = (int)(i / ((long long)nx * ny));
+            if (axis == 1) { f = y; t = z; }
+            else { f = z; t = y; }
+        } else {
+            const long long pid = i - n;
+            x = (int)(pid % nx);
+            t = (int)(pid / nx);
+            f = nsweep;
+        }
+        // 0-based linear index of rho3d(iaux, x', t') with the ghosted
+        // column x' = x + nb (+1 in Fortran) in the row slot (y sweep) or
+        // the plane slot (z sweep)
+        const long long rowplane = axis == 1 ? ((long long)(x + nb) + gy * (t + nb)) : ((long long)(t + nb) + gy * (x + nb));
+        double r[4], u[4];
+#pragma unroll
+        for (int o = 0; o < 4; ++o) {
+            const long long q = (long long)(f + nb - 3 + o) + gx * rowplane;  // iaux - 1 = f + nb + o - 3
+            if (q < 0 || q >= gtot) {
+                r[o] = u[o] = __longlong_as_double(0x7ff8000000000000ULL);
+                continue;
+            }
+            const long long a = q % gx, bq = (q / gx) % gy, cq = q / (gx * gy);
+            const long long ia = ((a - nb) % nx + nx) % nx;
+            const long long ib = ((bq - nb) % ny + ny) % ny;
+            const long long ic = ((cq - nb) % nz + nz) % nz;
+            const long long cell = ia + (long long)nx * (ib + (long long)ny * ic);
+            r[o] = rho[cell];
+            u[o] = vn[cell];
+        }
+        peak[i] = peak_value(r[0], r[1], r[2], r[3], u[1], u[2], dmax);
     }
 }
 
 __global__ void peak_prepass_kernel(const double* __restrict__ rho, const double* __restrict__ vn, double* peak,
-                                    int nx, int ny, int nz, int axis, double dmax, const DevCtl* c, int bslot) {
-    peak_prepass_box(rho, vn, peak, nx, ny, nz, axis, dmax, c, bslot,
+                                    int nx, int ny, int nz, int axis, double dmax, int nb, const DevCtl* c,
+                                    int bslot) {
+    peak_prepass_box(rho, vn, peak, nx, ny, nz, axis, dmax, nb, c, bslot,
                      blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
@@ -290,8 +329,9 @@ __global__ void peak_prepass_kernel(const double* __restrict__ rho, const double
 __global__ void peak_prepass_batch_kernel(BatchLaunch bl, int axis) {
     const SweepArgs& a = bl.args[bl.ent[blockIdx.y]];
     if (a.peak == nullptr) return;
-    peak_prepass_box(a.f[1], a.f[2], const_cast<double*>(a.peak), a.nx, a.ny, a.nz, axis, a.k.dmax, a.ctl, a.bslot,
-                     blockIdx.x * (long long)blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+    peak_prepass_box(a.f[1], a.f[2], const_cast<double*>(a.peak), a.nx, a.ny, a.nz, axis, a.k.dmax, a.k.nbound,
+                     a.ctl, a.bslot, blockIdx.x * (long long)blockDim.x + threadIdx.x,
+                     (long long)gridDim.x * blockDim.x);
 }
 
 int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st) {
@@ -303,7 +343,8 @@ int launch_peak_prepass_batch(const BatchLaunch& bl, int axis, cudaStream_t st) 
 int launch_peak_prepass(const Box& b, int axis, int bslot, cudaStream_t st) {
     if (axis == 0 || b.peak == nullptr) return 0;
     const double* vn = axis == 1 ? b.f[3] : b.f[4];
-    peak_prepass_kernel<<<592, 256, 0, st>>>(b.f[1], vn, b.peak, b.nx, b.ny, b.nz, axis, b.k.dmax, b.ctl, bslot);
+    peak_prepass_kernel<<<592, 256, 0, st>>>(b.f[1], vn, b.peak, b.nx, b.ny, b.nz, axis, b.k.dmax, b.k.nbound,
+                                             b.ctl, bslot);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
 }
 

@@ -2,16 +2,27 @@
 // kernels (internal; not part of the public header).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "hp_device.cuh"
 
 namespace hp {
 
+// NVTX range over a host-side scope (a sweep, a step, a batch step, a host
+// transfer): the timeline of a profiler groups the launches under it.  The
+// calls cost nothing measurable when no tool is attached.
+struct TraceRange {
+    explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange&) = delete;
+    TraceRange& operator=(const TraceRange&) = delete;
+};
+
 // One box resident on the device.
 struct Box {
     double* f[5];      // p, rho, vx, vy, vz (natural order), dense (nx,ny,nz), x fastest
     double* snap[4];   // step-start p, vx, vy, vz (cosmo expand), or null
-    double* peak;      // density-peak scratch for y/z sweeps (nx*ny*nz), or null
+    double* peak;      // density-peak values of the y/z faces (nx*ny*nz + nx*max(ny,nz)), or null
     double* g[3];      // gforce components x, y, z (dense, natural layout), or null: gravity off
     double* zlo;       // slab of a z-split box: 4 halo planes below, [p,rho,vx,vy,vz][4][nx*ny], or null
     double* zhi;       // 3 halo planes above, [5][3][nx*ny], or null

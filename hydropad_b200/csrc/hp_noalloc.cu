@@ -1,16 +1,16 @@
 // hp_noalloc.cu -- one directional sweep without any device allocation.
 //
-// Some callers cannot call cudaMalloc: code that runs inside a CUDA stream
-// capture that another component owns, allocators that forbid foreign
-// allocations (a framework's caching pool, an MPS/limited-memory client), or
-// a Fortran host that hands over device arrays it already owns and expects
-// the solver to add nothing to the device footprint.  hp_ppmsolver_noalloc
-// serves them: the caller passes the five state arrays (device memory), and
-// every scratch byte the sweep needs -- the control block with the time
-// scalars, the rho bounds and the status word, and the density-peak buffer
-// of the y/z sweeps -- lives in one file-scope __device__ array of a fixed
-// size, reserved once per device when the library's module is loaded and
-// held until the process exits.
+// Some callers cannot call cudaMalloc: a Fortran or C host that owns every
+// device array itself (its OpenACC or CUDA data regions hold the state) and
+// budgets the device memory on its own, a process whose device memory is
+// capped (an MPS client with a memory limit), or a framework whose caching
+// allocator owns the device and forbids foreign allocations.
+// hp_ppmsolver_noalloc serves them: the caller passes the five state arrays
+// (device memory), and every scratch byte the sweep needs -- the control
+// block with the time scalars, the rho bounds and the status word, and the
+// density-peak values of the y/z faces -- lives in one file-scope
+// __device__ array of a fixed size, reserved once per device when the
+// library's module is loaded and held until the process exits.
 //
 // The array is shared by every call: calls that overlap on the GPU (two
 // streams, or two host threads) race on it.  Each call re-initialises the
@@ -19,6 +19,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "../../include/hydropad_b200.h"
 #include "hp_device.cuh"
 #include "hp_launch.h"
@@ -26,18 +28,22 @@
 namespace {
 
 // Largest box the entry point accepts, in cells (1,048,576: e.g. 128x128x64
-// or 101^3).  The density-peak buffer needs one double per cell.
+// or 101^3).  The density-peak values need one double per cell plus one per
+// pencil of the y/z sweeps (at most cells/8, since every side is >= 8).
 constexpr long long kNoAllocMaxCells = 1LL << 20;
+constexpr long long kNoAllocPeakSlots = kNoAllocMaxCells + kNoAllocMaxCells / 8;
 constexpr size_t kCtlBytes = 4096;  // control block, padded
 static_assert(sizeof(hp::DevCtl) <= kCtlBytes, "control block does not fit");
 
-// The scratch array (8 MiB + 4 KiB per device).
-static __device__ __align__(256) unsigned char g_hp_noalloc_scratch[kCtlBytes + kNoAllocMaxCells * sizeof(double)];
+// The scratch array (9 MiB + 4 KiB per device).
+static __device__ __align__(256) unsigned char g_hp_noalloc_scratch[kCtlBytes + kNoAllocPeakSlots * sizeof(double)];
 
-// Device address of the array, per device ordinal; filled on first use.
-// In host code the symbol itself is only a host-side stand-in.
+// Device address of the array, per device ordinal; filled on the first call
+// with that device current.  In host code the symbol itself is only a
+// host-side stand-in.  Two host threads making their first call at once
+// both look the address up and store the same value.
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
+std::atomic<void*> g_scratch_addr[kMaxDevices];
 
 // Initialise the control block of this call from kernel arguments (no
 // memcpy from the host): time scalars, the bound slots, status and the
@@ -53,6 +59,7 @@ __global__ void noalloc_ctl_init(hp::DevCtl* c, hp::StepScalars s, double tstop)
         z.rho_key[q][0] = hp::kKeyPosInf;
         z.rho_key[q][1] = hp::kKeyNegInf;
     }
+    z.bad_cell = -1;
     *c = z;
 }
 
@@ -72,6 +79,7 @@ extern "C" int hp_ppmsolver_noalloc(double* p, double* rho, double* vx, double* 
     if (ndirection < 1 || ndirection > 3 || nx < 8 || ny < 8 || nz < 8) return HP_ERR_ARG;
     if ((long long)nx * ny * nz > kNoAllocMaxCells) return HP_ERR_ARG;  // larger than the static scratch
     if (params->precision != HP_PREC_FP64 && params->precision != HP_PREC_MIXED) return HP_ERR_ARG;
+    if (params->nbound < 3) return HP_ERR_ARG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return HP_ERR_NO_DEVICE;
     int major = 0;
@@ -79,12 +87,12 @@ extern "C" int hp_ppmsolver_noalloc(double* p, double* rho, double* vx, double* 
         return HP_ERR_NO_DEVICE;
     // First call on this device (with it current): look up the array's
     // device address.  Later calls reuse it.
-    if (!g_scratch_addr[dev]) {
-        void* addr = nullptr;
+    void* addr = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!addr) {
         if (cudaGetSymbolAddress(&addr, g_hp_noalloc_scratch) != cudaSuccess || !addr) return HP_ERR_CUDA;
-        g_scratch_addr[dev] = addr;
+        g_scratch_addr[dev].store(addr, std::memory_order_release);
     }
-    unsigned char* scratch = static_cast<unsigned char*>(g_scratch_addr[dev]);
+    unsigned char* scratch = static_cast<unsigned char*>(addr);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     hp::Box b;
@@ -117,6 +125,7 @@ extern "C" int hp_ppmsolver_noalloc(double* p, double* rho, double* vx, double* 
     k.dmax = params->dmax;
     k.eta1 = params->eta1;
     k.eta2 = params->eta2;
+    k.nbound = params->nbound;
     k.nroot = 0;
     k.jrg = 0;
     const double n = k.rm, j = k.rgamma * k.rm;

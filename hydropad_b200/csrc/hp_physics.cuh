@@ -31,6 +31,9 @@ struct Consts {
     double mingradflat, flatvalue, dmax, eta1, eta2, dx, rdx;
     int nroot;  // 1/m when it is an integer in [2, 9] (5 for gamma = 5/3), else 0
     int jrg;    // rgamma/m when nroot != 0 and it is an integer in [1, 9], else 0
+    int nbound; // ghost layers of the reference's arrays (&MESH nbound): only the
+                // y/z density-peak gather, which indexes those arrays, depends on it
+    int pad_;
 };
 struct StepScalars {
     double dt, rdtath, at, dat, rat, ath, dath;

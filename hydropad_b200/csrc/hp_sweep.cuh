@@ -320,8 +320,13 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
             kvel = kb > kvel ? kb : kvel;
         }
-        if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) status |= kStatNaN;
-        else if (rho <= 0.0 || p <= 0.0) status |= kStatNegative;
+        if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) {
+            status |= kStatNaN;
+            record_bad_cell(a.ctl, g);
+        } else if (rho <= 0.0 || p <= 0.0) {
+            status |= kStatNegative;
+            record_bad_cell(a.ctl, g);
+        }
     };
 
     for (int b = -4; b <= N + 3 + kLag; b += T, par ^= 1) {
@@ -620,10 +625,13 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 } else {
                     // the reference gathers these with the x index slot
                     // (ppmsolver.F90:251-252, 379-380); a pre-pass has
-                    // evaluated them on the pre-sweep state
-                    const long long wbase = pencil_base<AXIS>(pid0 + wtp, a.nx, a.ny);
-                    const int fw = f < N ? f : f - N;
-                    pk = a.peak[wbase + stride * fw];
+                    // evaluated them on the pre-sweep state: face f < N at
+                    // the index of cell f, face N after the last cell
+                    if (f < N) {
+                        pk = a.peak[pencil_base<AXIS>(pid0 + wtp, a.nx, a.ny) + stride * f];
+                    } else {
+                        pk = a.peak[(long long)a.nx * a.ny * a.nz + pid0 + wtp];
+                    }
                 }
                 out.p = fmax2(out.p, pk);
             }

@@ -8,6 +8,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "hp_launch.h"
 #include "hp_sweep.cuh"
 
@@ -44,17 +46,32 @@ static inline SweepArgs make_sweep_args(const Box& b, int axis, int bslot, int f
     return a;
 }
 
+// The dynamic shared-memory size of a kernel above 48 KB must be allowed on
+// every device that launches it: one bit per device ordinal, per kernel.
+// Two host threads that race here both set the attribute (harmless).
+static inline int current_device() {
+    int dev = 0;
+    return cudaGetDevice(&dev) == cudaSuccess ? dev : -1;
+}
+template <class Kern>
+static bool allow_smem(Kern kern, size_t smem, std::atomic<unsigned long long>& done_mask) {
+    const int dev = current_device();
+    if (dev < 0 || dev >= 64) return false;
+    const unsigned long long bit = 1ULL << dev;
+    if (done_mask.load(std::memory_order_acquire) & bit) return true;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return false;
+    done_mask.fetch_or(bit, std::memory_order_acq_rel);
+    return true;
+}
+
 template <int AXIS, int P, int T, int RING, class Policy, int MINB = 1, bool GRAV = false, bool PENCIL = false>
 static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
     const SweepArgs a = make_sweep_args(b, AXIS, bslot, flags);
     const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy, GRAV, PENCIL>);
     auto kern = ppm_sweep_kernel<AXIS, P, T, RING, Policy, MINB, GRAV, PENCIL>;
-    static bool attr_set = false;  // per instantiation (one process drives one device)
-    if (!attr_set) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return -1;
-        attr_set = true;
-    }
+    static std::atomic<unsigned long long> attr_mask{0};  // per instantiation, one bit per device
+    if (!allow_smem(kern, smem, attr_mask)) return -1;
     const long long grid = (a.npencil + P - 1) / P;
     kern<<<(unsigned)grid, P * T, smem, st>>>(a);
     return cudaPeekAtLastError() == cudaSuccess ? 1 : -1;
@@ -99,15 +116,18 @@ template <int AXIS, int P, int T, int RING, class Policy, int MINB>
 static int launch_sweep_batch_t(const BatchLaunch& bl, cudaStream_t st) {
     const size_t smem = sizeof(SweepSmem<AXIS, P, T, RING, Policy>);
     auto kern = ppm_sweep_batch_kernel<AXIS, P, T, RING, Policy, MINB>;
-    static int grid = 0;  // per instantiation (one process drives one device)
+    // per instantiation and device: the attribute, then the resident grid
+    static std::atomic<unsigned long long> attr_mask{0};
+    static std::atomic<int> grids[64];
+    if (!allow_smem(kern, smem, attr_mask)) return -1;
+    const int dev = current_device();
+    int grid = grids[dev].load(std::memory_order_acquire);
     if (grid == 0) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return -1;
-        int dev = 0, sms = 0, per_sm = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+        int sms = 0, per_sm = 0;
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, P * T, smem) != cudaSuccess) return -1;
         grid = sms * (per_sm > 0 ? per_sm : 1);
+        grids[dev].store(grid, std::memory_order_release);
     }
     const int g = bl.nitems < grid ? bl.nitems : grid;
     if (g <= 0) return 0;

@@ -179,16 +179,21 @@ int hp_get_tiles(hp_ctx *ctx, int *tiles /* [3] */);
 int hp_autotune(hp_ctx *ctx, int reps);
 
 /* One directional sweep (1=x, 2=y, 3=z) on caller-owned DEVICE arrays,
- * without any device allocation, for callers that cannot allocate (a stream
- * capture owned by someone else, a foreign memory pool, a host that owns all
- * device memory).  No counterpart in the reference.
+ * without any device allocation, for callers that cannot allocate: a host
+ * that owns every device array and budgets device memory itself (its
+ * OpenACC or CUDA data regions hold the state), a process whose device
+ * memory is capped, or a framework whose caching allocator owns the device.
+ * No counterpart in the reference.
  *   p..vz: device pointers, dense (nx,ny,nz) interior cells, x fastest,
- *          periodic; updated in place.  params: namelist values and
- *          precision; scalars: dt, rdtath, at, dat, rat, ath, dath.
+ *          periodic; updated in place.  params: namelist values (nbound >= 3:
+ *          the ghost layers of the reference's arrays, which the y/z
+ *          density-peak test indexes) and precision; scalars: dt, rdtath,
+ *          at, dat, rat, ath, dath.
  *   stream: cudaStream_t (NULL: default stream); the call returns after the
  *          stream has finished the sweep.
- * All scratch (control block + density-peak buffer) is one static device
- * array of 8 MiB + 4 KiB held by every device that loads the library, so
+ * It takes no gforce: the sweep runs without the gravity source.
+ * All scratch (control block + density-peak values) is one static device
+ * array of 9 MiB + 4 KiB held by every device that loads the library, so
  * nx*ny*nz may not exceed 1,048,576 cells (HP_ERR_ARG beyond).  The first
  * call on a device looks up the array's address (cudaGetSymbolAddress);
  * make that first call before any stream capture.  Calls share the array:
@@ -300,6 +305,13 @@ int hp_step_finish(hp_ctx *ctx, double velmax);
 /* Block until the context's stream is idle and return the device status
  * word accumulated since the last call (then cleared). */
 int hp_synchronize(hp_ctx *ctx);
+
+/* Dense index (x + nx*(y + ny*z)) of the first updated cell that the last
+ * non-zero status word read by hp_synchronize / hp_evolve reported (NaN, or
+ * a non-positive density or pressure), or -1.  No counterpart in the
+ * reference, which stops with a message only for Newton failures
+ * (riemann.F90:62-65). */
+long long hp_bad_cell(hp_ctx *ctx);
 
 /* CUDA stream the context launches on (cudaStream_t), for event timing. */
 void *hp_stream(hp_ctx *ctx);

@@ -288,9 +288,9 @@ def test_config1_sod64(oracle):
     assert abs(g.t - s.t) <= 1e-12 * s.t
 
 
-def test_config2_eds256_fp64_two_steps(oracle):
-    """The cosmological configuration at its full size (256^3): two steps of
-    the FP64 path against the oracle (parity at the size the bench runs)."""
+def test_config2_eds256_fp64_ten_steps(oracle):
+    """The cosmological configuration at its full size (256^3): ten steps of
+    the FP64 path against the oracle, the north star's FP64 gate."""
     n = 256
     state = grf_state(n, seed=12345)
     prm = params_for((n, n, n), cosmo=True)
@@ -300,7 +300,35 @@ def test_config2_eds256_fp64_two_steps(oracle):
     with _hydro(prm) as h:
         h.attach_state(*state)
         _copy_scalars(h, s)
-        h.evolve(2, graph=True)
+        h.evolve(10, graph=True)
         out = h.download()
-    assert st.evolve(s, 2) == 0
-    _assert_fields(out, st.f, FP64_TOL, "EdS 256^3, 2 steps")
+        g = h.get_scalars()
+    assert st.evolve(s, 10) == 0
+    _assert_fields(out, st.f, FP64_TOL, "EdS 256^3, 10 steps")
+    assert abs(g.t - s.t) <= 1e-12 * abs(s.t)
+
+
+def test_config2_eds256_runs_to_z10():
+    """The cosmological configuration runs from z = 50 to z = 10 (tstop,
+    initialize_parameters.F90:85) and stops there: the step count and the
+    final expansion factor of the FP64 and mixed paths."""
+    n = 256
+    state = grf_state(n, seed=12345)
+    prm = params_for((n, n, n), cosmo=True)
+    steps = {}
+    for prec in ("fp64", "mixed"):
+        with _hydro(prm, prec) as h:
+            h.attach_state(*state)
+            h.start_with_cfl()
+            done = 0
+            while done < 200:
+                h.evolve(1, graph=True)
+                done += 1
+                g = h.get_scalars()
+                if not g.told < prm.tstop:
+                    break
+            a_end = g.t ** (2.0 / 3.0)
+            steps[prec] = g.nstep - 1
+        assert abs(a_end - 1.0 / 11.0) <= 1e-9, (prec, a_end)
+    assert all(50 <= v <= 200 for v in steps.values()), steps
+    print(f"steps from z=50 to z=10 at 256^3: {steps}")

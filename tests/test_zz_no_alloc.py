@@ -1,11 +1,15 @@
 """hp_ppmsolver_noalloc: the sweep for callers that cannot allocate device
-memory (a stream capture owned by another component, a foreign memory
-pool, a host that owns every device array).  The caller passes the state
-arrays; the scratch lives in a static device array inside the library.
+memory -- a host that owns every device array and budgets device memory
+itself, a process whose device memory is capped, or a framework whose
+caching allocator owns the device.  The caller passes the state arrays; the
+scratch lives in a static device array inside the library.
 
 Checked against the allocating entry point (hp_ppmsolver on an attached
-context) on two calls in a row, with the single-sweep tolerance the parity
-tests use.  Collected last on purpose (file name), so a failure here comes
+context) on three calls in a row (x, y, z sweeps), with the single-sweep
+tolerance the parity tests use: on a cosmological box, and on a non-cubic
+box with density spikes and a low dmax, where the y/z sweeps run the
+density-peak pre-pass (its values occupy the second part of the static
+array).  Collected last on purpose (file name), so a failure here comes
 after every other test has run.
 """
 import ctypes as C
@@ -40,16 +44,24 @@ def _params_struct(h):
     return p
 
 
+@pytest.mark.parametrize("case", ["grf", "peak"])
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
-def test_noalloc_matches_allocating_entry_point(prec):
+def test_noalloc_matches_allocating_entry_point(prec, case):
     import torch
 
     from hydropad_b200 import _lib as L
     from hydropad_b200.api import Hydro
 
-    n = 32
-    state = grf_state(n, seed=29)
-    prm = params_for((n, n, n), cosmo=True)
+    if case == "grf":
+        shape = (32, 32, 32)
+        state = grf_state(32, seed=29)
+        prm = params_for(shape, cosmo=True)
+    else:
+        from tests.test_gpu_peak import spiky_state
+        shape = (32, 24, 40)
+        state = spiky_state(shape, seed=31)
+        prm = params_for(shape, dmax=1.5)
+    nx, ny, nz = shape
     with Hydro(prm, precision=prec) as h:
         h.attach_state(*state)
         h.start_with_cfl()
@@ -57,10 +69,10 @@ def test_noalloc_matches_allocating_entry_point(prec):
         pstruct = _params_struct(h)
         dev = [torch.from_numpy(_dense(a)).cuda() for a in state]  # p, rho, vx, vy, vz
         torch.cuda.synchronize()
-        for call, nd in enumerate((1, 2)):  # two calls in a row
+        for call, nd in enumerate((1, 2, 3)):  # three calls in a row
             h.ppmsolver(nd)
             ref = h.download()
-            rc = L.lib().hp_ppmsolver_noalloc(*[C.c_void_p(t.data_ptr()) for t in dev], n, n, n, nd,
+            rc = L.lib().hp_ppmsolver_noalloc(*[C.c_void_p(t.data_ptr()) for t in dev], nx, ny, nz, nd,
                                               C.byref(pstruct), C.byref(scal), None)
             assert rc == 0, L.lib().hp_strerror(rc)
             for q in range(5):
@@ -70,7 +82,7 @@ def test_noalloc_matches_allocating_entry_point(prec):
                     assert np.abs(got).max() == 0.0
                     continue
                 e = rel_l1(got, want)
-                assert e <= SWEEP_TOL, (prec, call, q, e)
+                assert e <= SWEEP_TOL, (prec, case, call, q, e)
 
 
 def test_noalloc_rejects_boxes_beyond_its_scratch():
