@@ -14,7 +14,7 @@ HP_OK = 0
 HP_ERR = {
     -1: "HP_ERR_ARG", -2: "HP_ERR_CUDA", -3: "HP_ERR_OOM", -4: "HP_ERR_NEWTON", -5: "HP_ERR_NAN",
     -6: "HP_ERR_NEGATIVE_STATE", -7: "HP_ERR_NOT_ATTACHED", -8: "HP_ERR_STATE_MISMATCH", -9: "HP_ERR_NO_DEVICE",
-    -10: "HP_ERR_UNSUPPORTED",
+    -10: "HP_ERR_UNSUPPORTED", -11: "HP_ERR_TIMEOUT",
 }
 HP_PREC_FP64 = 0
 HP_PREC_MIXED = 1

@@ -44,8 +44,8 @@ SOURCES = [
     ("hp_batch.cu", []),
     ("hp_noalloc.cu", []),
 ]
-HEADERS = ["hp_physics.cuh", "hp_riemann.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_sweep_launch.cuh",
-           "hp_launch.h", "hp_ctx.h"]
+HEADERS = ["hp_physics.cuh", "hp_riemann.cuh", "hp_device.cuh", "hp_sweep.cuh", "hp_sweep_ws.cuh", "hp_tma.cuh",
+           "hp_sweep_launch.cuh", "hp_launch.h", "hp_ctx.h"]
 
 
 def _nvcc() -> str:

@@ -407,8 +407,8 @@ int hp_batch_synchronize(hp_batch* b, int* status) {
 int hp_batch_set_tiles(hp_batch* b, int tile_x, int tile_y, int tile_z) {
     if (!b) return HP_ERR_ARG;
     const int t[3] = {tile_x, tile_y, tile_z};
-    for (int a = 0; a < 3; ++a)
-        if (t[a] < 0 || t[a] >= hp::kNumTiles) return HP_ERR_ARG;
+    for (int a = 0; a < 3; ++a)  // the batched kernel runs the classic tiles
+        if (t[a] < 0 || t[a] >= hp::kNumClassicTiles) return HP_ERR_ARG;
     HP_CUDA(cudaSetDevice(b->dev));
     HP_CUDA(cudaStreamSynchronize(b->stream));
     for (int a = 0; a < 3; ++a) b->tile[a] = t[a];
@@ -466,7 +466,7 @@ int hp_batch_autotune(hp_batch* b, int reps) {
                                        b->stream));
     }
     for (int axis = 0; axis < 3 && rc == HP_OK; ++axis) {
-        for (int tile = 0; tile < hp::kNumTiles && rc == HP_OK; ++tile) {
+        for (int tile = 0; tile < hp::kNumClassicTiles && rc == HP_OK; ++tile) {
             const int P_ = hp::kTilePencils[axis][tile];
             plan.assign(2 * n + 1, 0);
             int first = 0;

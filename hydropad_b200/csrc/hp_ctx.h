@@ -37,6 +37,7 @@ constexpr int kSweepOrder[6][3] = {{0, 1, 2}, {2, 1, 0}, {1, 2, 0}, {0, 2, 1}, {
 
 // Error code of a device status word.
 inline int status_error(unsigned st) {
+    if (st & kStatTimeout) return HP_ERR_TIMEOUT;
     if (st & kStatNewton) return HP_ERR_NEWTON;
     if (st & kStatNaN) return HP_ERR_NAN;
     if (st & kStatNegative) return HP_ERR_NEGATIVE_STATE;

@@ -13,6 +13,7 @@ enum : unsigned {
     kStatNaN = 2u,       // NaN in an updated cell
     kStatNegative = 4u,  // rho <= 0 or p <= 0 in an updated cell
     kStatUnsupported = 8u,  // a case the sweep cannot take (the density-peak fix across z slabs)
+    kStatTimeout = 16u,     // a bounded wait of the pipelined sweep gave up (its results are void)
 };
 
 // Sweep flags.

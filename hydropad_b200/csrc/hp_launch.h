@@ -41,9 +41,14 @@ int launch_speed(const Box& b, cudaStream_t st);
 int launch_timedet(const Box& b, int advance, cudaStream_t st);
 
 // Number of tile shapes per axis, and the pencils per CTA (P) of each
-// (the tile table in hp_sweep_launch.cuh).
-constexpr int kNumTiles = 11;
-constexpr int kTilePencils[3][kNumTiles] = {{8, 4, 8, 4, 16, 12, 8, 4, 8, 4, 16},
+// (the tile tables in hp_sweep_launch.cuh): tiles 0 .. kNumClassicTiles-1
+// run ppm_sweep_kernel (and the batched kernel), the others the pipelined
+// ppm_sweep_ws_kernel (single boxes; a box it does not take -- gravity, the
+// full-pencil solver, a z slab, a row length it cannot tile -- runs tile 0).
+constexpr int kNumClassicTiles = 11;
+constexpr int kNumWsTiles = 3;
+constexpr int kNumTiles = kNumClassicTiles + kNumWsTiles;
+constexpr int kTilePencils[3][kNumClassicTiles] = {{8, 4, 8, 4, 16, 12, 8, 4, 8, 4, 16},
                                             {32, 16, 32, 16, 64, 32, 32, 16, 32, 16, 16},
                                             {32, 16, 32, 16, 64, 32, 32, 16, 32, 16, 16}};
 

@@ -180,6 +180,209 @@ __device__ __forceinline__ void pencil_sync() {
     else __syncthreads();
 }
 
+// ---------------------------------------------------------------------------
+// Per-cell stage bodies shared by the sweep kernels (every kernel computes a
+// cell's values with these, so they agree bit for bit).
+// ---------------------------------------------------------------------------
+
+// Stage A of cell c from cells c-1, c, c+1 (p, rho, u, v, w): the ajside
+// slopes, the dda second difference of rho and the flattening flag of the
+// pair (c, c+1) (order2interp.F90:65-113, ppm_functs.F90:167-181, dda.F90:17).
+template <class R>
+__device__ __forceinline__ void slopes_of_cell(const R am[5], const R a0[5], const R ap[5], R ming, R dx, R sl[5],
+                                               R& d2, bool& flag) {
+    flag = false;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        sl[q] = ajside<R>(am[q], a0[q], ap[q]);
+        flag |= flat_pair<R>(a0[q], ap[q], ming);
+        if (q == 1) d2 = dda_second<R>(am[q], a0[q], ap[q], dx);
+    }
+}
+
+// Time scalars of the reconstruction, in its type.
+template <class R>
+struct TraceScalars {
+    R dt, rat, dat, at, dx, gam, flatv;
+};
+
+// Stage B of cell c: flattening, the five parabolas (monotonicity, contact
+// steepening of rho, flattening) and the characteristic tracing in expanding
+// coordinates (order2interp.F90:115-258, ppm_functs.F90:1-162).  q1..q3 are
+// cells c-1, c, c+1, dm..dp their slopes, Dm/Dp the second differences of
+// rho at c-1 and c+1, fl_any the flattening flags of the pairs c-2 .. c+1.
+// Gravity: g1..g3 = -gforce of cells c-1..c+1 and their slopes.  Returns the
+// traced left state of face c+1 (`left`) and the right state of face c.
+template <class R, bool GRAV, bool PENCIL>
+__device__ __forceinline__ void trace_cell(const R q1[5], const R q2[5], const R q3[5], const R dm[5], const R d0[5],
+                                           const R dp[5], R Dm, R Dp, bool fl_any, R g1, R g2, R g3, R gdm, R gd0,
+                                           R gdp, const TraceScalars<R>& ts, R left[5], FaceState& right) {
+    const R dt_ = ts.dt, rat_ = ts.rat, dat_ = ts.dat, at_ = ts.at, dx_ = ts.dx, gam_ = ts.gam;
+    const R flat = fl_any ? ts.flatv : R(0);
+    const R pm1 = q1[0], p0 = q2[0], pp1 = q3[0];
+    const R rm1 = q1[1], r0 = q2[1], rp1 = q3[1];
+    const R addp = fabs(pp1 - pm1) / fmin2(pm1, pp1);
+    const R addrho = R(0.5) * gam_ * fabs(rp1 - rm1) / fmin2(rm1, rp1);
+    const bool steep = addrho >= addp;
+    const R u0 = q2[2];
+    // sound speed of the characteristic speeds: the cell's own
+    // (order2interp.F90:56-57); the full-pencil solver takes the next
+    // cell's (ppm.F90:106-107: cbar = c(i), c(i+1) beside vxbar(2),
+    // vxbar(3) = cells i-1, i)
+    const R cc = PENCIL ? sqrt(gam_ * pp1 / rp1) : sqrt(gam_ * p0 / r0);
+    // characteristic speeds of the cell (order2interp.F90:194-196,221-223)
+    const R lm = (u0 - cc) * rat_, l0 = u0 * rat_, lp = (u0 + cc) * rat_;
+    // x = y/dx of fl/fr (ppm_functs.F90:59-84); the right-side arguments
+    // are exact negations of the left-side ones.
+    const R yp = dt_ * (u0 + cc) * rat_;
+    const R ym = dt_ * (u0 - cc) * rat_;
+    const R y0 = dt_ * u0 * rat_;
+    const R xp = yp / dx_, xm = ym / dx_, x0 = y0 / dx_;
+    const R xtl = (R(0) > yp) ? R(0) / dx_ : xp;    // max(cv,0), atl
+    const R xtr = (R(0) > -ym) ? R(0) / dx_ : -xm;  // max(cv,0), atr
+    // traced values (t: fl/fr at the face; 1,2,3: the -,0,+
+    // characteristics).  All are evaluated, branch-free; the tracing below
+    // selects the ones the reference computes.
+    R ptl, pc1l, pc2l, pc3l, ptr, pc1r, pc2r, pc3r;
+    R rtl, rc2l, rtr, rc2r;
+    R utl, uc1l, uc3l, utr, uc1r, uc3r;
+    R vtl, vc2l, vtr, vc2r, wtl, wc2l, wtr, wc2r;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        R Dmq = 0, Dpq = 0;
+        const bool st = (q == 1) && steep;
+        if (q == 1) { Dmq = Dm; Dpq = Dp; }
+        const Parabola<R> Pq = build_parabola<R>(q1[q], q2[q], q3[q], dm[q], d0[q], dp[q], flat, st, Dmq, Dpq, dx_);
+        const R tl_ = fl(Pq, xtl), tr_ = fr(Pq, xtr);
+        if (q == 0) {
+            ptl = tl_; ptr = tr_;
+            pc1l = fl(Pq, xm); pc2l = fl(Pq, x0); pc3l = fl(Pq, xp);
+            pc1r = fr(Pq, -xm); pc2r = fr(Pq, -x0); pc3r = fr(Pq, -xp);
+        } else if (q == 1) {
+            rtl = tl_; rtr = tr_;
+            rc2l = fl(Pq, x0); rc2r = fr(Pq, -x0);
+        } else if (q == 2) {
+            utl = tl_; utr = tr_;
+            uc1l = fl(Pq, xm); uc3l = fl(Pq, xp);
+            uc1r = fr(Pq, -xm); uc3r = fr(Pq, -xp);
+        } else if (q == 3) {
+            vtl = tl_; vtr = tr_;
+            vc2l = fl(Pq, x0); vc2r = fr(Pq, -x0);
+        } else {
+            wtl = tl_; wtr = tr_;
+            wc2l = fl(Pq, x0); wc2r = fr(Pq, -x0);
+        }
+    }
+    // negative traced states (order2interp.F90:174-190)
+    if (ptl < R(0)) ptl = R(kTiny);
+    if (ptr < R(0)) ptr = R(kTiny);
+    if (rtl < R(0)) rtl = R(kTiny);
+    if (rtr < R(0)) rtr = R(kTiny);
+    // g at the -/+ characteristics (order2interp.F90:170-172); gravity
+    // off: g == 0
+    R gc1l = R(0), gc3l = R(0), gc1r = R(0), gc3r = R(0);
+    if constexpr (GRAV) {
+        const Parabola<R> Pg = build_parabola<R>(g1, g2, g3, gdm, gd0, gdp, flat, false, R(0), R(0), dx_);
+        gc1l = fl(Pg, xm);
+        gc3l = fl(Pg, xp);
+        gc1r = fr(Pg, -xm);
+        gc3r = fr(Pg, -xp);
+    }
+    // left state of face c+1 (order2interp.F90:192-219,249-258)
+    {
+        const R ctl = sqrt(gam_ * ptl * rtl);
+        const R bm_ = beta<R>(ctl, utl, uc1l, ptl, pc1l, gc1l, R(-1), dt_, at_, dat_, rat_);
+        const R bp_ = beta<R>(ctl, utl, uc3l, ptl, pc3l, gc3l, R(1), dt_, at_, dat_, rat_);
+        const R b0_ = beta0<R>(ctl, rtl, rc2l, ptl, pc2l, dt_, at_, dat_);
+        const R bml = (lm > R(0)) ? bm_ : R(0);
+        const R bpl = (lp > R(0)) ? bp_ : R(0);
+        const R b0l = (l0 > R(0)) ? b0_ : R(0);
+        const R vl = (l0 > R(0)) ? vc2l : vtl;
+        const R wl = (l0 > R(0)) ? wc2l : wtl;
+        R pl = ptl + ctl * ctl * (bpl + bml);
+        if (pl <= R(0)) pl = ptl;
+        const R ul = utl + ctl * (bpl - bml);
+        R rl = R(1) / (R(1) / rtl - bml - b0l - bpl);
+        if (rl <= R(0)) rl = rtl;
+        left[0] = pl;
+        left[1] = rl;
+        left[2] = ul;
+        left[3] = vl;
+        left[4] = wl;
+    }
+    // right state of face c (order2interp.F90:221-258)
+    {
+        const R ctr = sqrt(gam_ * ptr * rtr);
+        const R bp_ = beta<R>(ctr, utr, uc3r, ptr, pc3r, gc3r, R(1), dt_, at_, dat_, rat_);
+        const R bm_ = beta<R>(ctr, utr, uc1r, ptr, pc1r, gc1r, R(-1), dt_, at_, dat_, rat_);
+        const R b0_ = beta0<R>(ctr, rtr, rc2r, ptr, pc2r, dt_, at_, dat_);
+        const R bpr = (lp < R(0)) ? bp_ : R(0);
+        const R bmr = (lm < R(0)) ? bm_ : R(0);
+        const R b0r = (l0 < R(0)) ? b0_ : R(0);
+        const R vr = (l0 < R(0)) ? vc2r : vtr;
+        const R wr = (l0 < R(0)) ? wc2r : wtr;
+        R pr = ptr + ctr * ctr * (bpr + bmr);
+        if (pr <= R(0)) pr = ptr;
+        const R ur = utr + ctr * (bpr - bmr);
+        R rr = R(1) / (R(1) / rtr - bmr - b0r - bpr);
+        if (rr <= R(0)) rr = rtr;
+        right.p = pr;
+        right.rho = rr;
+        right.u = ur;
+        right.v = vr;
+        right.w = wr;
+    }
+}
+
+// Stage D's epilogue for cell g (updated state p, rho, u, v, w): expand
+// with the step-start snapshot (expand.F90:18-41), the store, and the
+// step's reductions (rho bounds, speed.F90:25-28 velmax, status).
+template <int AXIS>
+__device__ __forceinline__ void finish_cell(const SweepArgs& a, long long g, double p, double rho, double u, double v,
+                                            double w, double afact, double afact1, double afact2,
+                                            unsigned long long& kmin, unsigned long long& kmax,
+                                            unsigned long long& kvel, unsigned& status) {
+    if (a.flags & kFlagExpand) {
+        const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
+        const double vx_o = zero_old ? 0.0 : a.snap[1][g];
+        const double vy_o = zero_old ? 0.0 : a.snap[2][g];
+        const double vz_o = zero_old ? 0.0 : a.snap[3][g];
+        const double p_o = zero_old ? 0.0 : a.snap[0][g];
+        const double un_o = AXIS == 0 ? vx_o : (AXIS == 1 ? vy_o : vz_o);
+        const double v_o = AXIS == 0 ? vy_o : (AXIS == 1 ? vx_o : vy_o);
+        const double w_o = AXIS == 0 ? vz_o : (AXIS == 1 ? vz_o : vx_o);
+        u = (2.0 * u - afact * un_o) * afact2;
+        v = (2.0 * v - afact * v_o) * afact2;
+        w = (2.0 * w - afact * w_o) * afact2;
+        const double ppp = p;
+        p = (p - afact * p_o) * afact1;
+        if (p <= 0.0) p = ppp > 0.0 ? ppp : p_o;
+    }
+    a.f[0][g] = p;
+    a.f[1][g] = rho;
+    a.f[2][g] = u;
+    a.f[3][g] = v;
+    a.f[4][g] = w;
+    const unsigned long long kr = dkey(rho);
+    kmin = kr < kmin ? kr : kmin;
+    kmax = kr > kmax ? kr : kmax;
+    if (a.flags & kFlagSpeed) {
+        const double vs = sqrt(a.k.gamma * p / rho);
+        double vm = fabs(u) + vs;
+        vm = fmax2(vm, fabs(v) + vs);
+        vm = fmax2(vm, fabs(w) + vs);
+        const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
+        kvel = kb > kvel ? kb : kvel;
+    }
+    if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) {
+        status |= kStatNaN;
+        record_bad_cell(a.ctl, g);
+    } else if (rho <= 0.0 || p <= 0.0) {
+        status |= kStatNegative;
+        record_bad_cell(a.ctl, g);
+    }
+}
+
 // One CTA's worth of work: the P pencils pid0 .. pid0+P-1 of the box `a`,
 // walked from end to end.  Every thread of the CTA calls it.
 // PENCIL: the non-STENCIL build's full-pencil solver (hydro/ppm.F90)
@@ -214,6 +417,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     const StepScalars sc = a.ctl->s;
     const R dt_ = R(sc.dt), rat_ = R(sc.rat), dat_ = R(sc.dat), at_ = R(sc.at);
     const R dx_ = R(k.dx), gam_ = R(k.gamma), flatv_ = R(k.flatvalue), ming_ = R(k.mingradflat);
+    const TraceScalars<R> ts{dt_, rat_, dat_, at_, dx_, gam_, flatv_};
     if (a.ctl->done) return;  // told >= tstop: the time loop has ended (main.F90:100)
 
     // density-peak fix is possible only if some rho exceeds dmax x another
@@ -285,48 +489,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         }
     };
     // D's epilogue: expand, store, and the step's reductions
-    auto finish_cell = [&](long long g, double p, double rho, double u, double v, double w) {
-        if (a.flags & kFlagExpand) {
-            // expand.F90:22-41 with the step-start snapshot
-            const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
-            const double vx_o = zero_old ? 0.0 : a.snap[1][g];
-            const double vy_o = zero_old ? 0.0 : a.snap[2][g];
-            const double vz_o = zero_old ? 0.0 : a.snap[3][g];
-            const double p_o = zero_old ? 0.0 : a.snap[0][g];
-            const double un_o = AXIS == 0 ? vx_o : (AXIS == 1 ? vy_o : vz_o);
-            const double v_o = AXIS == 0 ? vy_o : (AXIS == 1 ? vx_o : vy_o);
-            const double w_o = AXIS == 0 ? vz_o : (AXIS == 1 ? vz_o : vx_o);
-            u = (2.0 * u - afact * un_o) * afact2;
-            v = (2.0 * v - afact * v_o) * afact2;
-            w = (2.0 * w - afact * w_o) * afact2;
-            const double ppp = p;
-            p = (p - afact * p_o) * afact1;
-            if (p <= 0.0) p = ppp > 0.0 ? ppp : p_o;
-        }
-        a.f[0][g] = p;
-        a.f[1][g] = rho;
-        a.f[2][g] = u;
-        a.f[3][g] = v;
-        a.f[4][g] = w;
-        const unsigned long long kr = dkey(rho);
-        kmin = kr < kmin ? kr : kmin;
-        kmax = kr > kmax ? kr : kmax;
-        if (a.flags & kFlagSpeed) {
-            // speed.F90:25-28
-            const double vs = sqrt(k.gamma * p / rho);
-            double vm = fabs(u) + vs;
-            vm = fmax2(vm, fabs(v) + vs);
-            vm = fmax2(vm, fabs(w) + vs);
-            const unsigned long long kb = (unsigned long long)__double_as_longlong(vm);
-            kvel = kb > kvel ? kb : kvel;
-        }
-        if (!(rho == rho) || !(p == p) || !(u == u) || !(v == v) || !(w == w)) {
-            status |= kStatNaN;
-            record_bad_cell(a.ctl, g);
-        } else if (rho <= 0.0 || p <= 0.0) {
-            status |= kStatNegative;
-            record_bad_cell(a.ctl, g);
-        }
+    auto finish = [&](long long g, double p, double rho, double u, double v, double w) {
+        finish_cell<AXIS>(a, g, p, rho, u, v, w, afact, afact1, afact2, kmin, kmax, kvel, status);
     };
 
     for (int b = -4; b <= N + 3 + kLag; b += T, par ^= 1) {
@@ -388,14 +552,18 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             const int c = ew - 1;
             if (activew && c >= -3 && c <= N + 1) {
                 const int im = L::idx(c - 1, tpw), i0 = L::idx(c, tpw), ip = L::idx(c + 1, tpw);
-                bool flag = false;
+                R am[5], a0[5], ap[5], sl[5], d2;
+                bool flag;
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
-                    const R am = R(S.st[q][im]), a0 = R(S.st[q][i0]), ap = R(S.st[q][ip]);
-                    S.sl[q][i0] = ajside<R>(am, a0, ap);
-                    flag |= flat_pair<R>(a0, ap, ming_);
-                    if (q == 1) S.d2[i0] = dda_second<R>(am, a0, ap, dx_);
+                    am[q] = R(S.st[q][im]);
+                    a0[q] = R(S.st[q][i0]);
+                    ap[q] = R(S.st[q][ip]);
                 }
+                slopes_of_cell<R>(am, a0, ap, ming_, dx_, sl, d2, flag);
+#pragma unroll
+                for (int q = 0; q < 5; ++q) S.sl[q][i0] = sl[q];
+                S.d2[i0] = d2;
                 S.pf[i0] = flag ? 1 : 0;
                 if constexpr (GRAV) S.slg[i0] = ajside<R>(R(S.sg[im]), R(S.sg[i0]), R(S.sg[ip]));
             }
@@ -409,125 +577,26 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
 #pragma unroll
                 for (int o = 0; o < 5; ++o) ic[o] = L::idx(c - 2 + o, tpw);
                 const bool fl_any = S.pf[ic[0]] | S.pf[ic[1]] | S.pf[ic[2]] | S.pf[ic[3]];
-                const R flat = fl_any ? flatv_ : R(0);
-                const R pm1 = R(S.st[0][ic[1]]), p0 = R(S.st[0][ic[2]]), pp1 = R(S.st[0][ic[3]]);
-                const R rm1 = R(S.st[1][ic[1]]), r0 = R(S.st[1][ic[2]]), rp1 = R(S.st[1][ic[3]]);
-                const R addp = fabs(pp1 - pm1) / fmin2(pm1, pp1);
-                const R addrho = R(0.5) * gam_ * fabs(rp1 - rm1) / fmin2(rm1, rp1);
-                const bool steep = addrho >= addp;
-                const R u0 = R(S.st[2][ic[2]]);
-                // sound speed of the characteristic speeds: the cell's own
-                // (order2interp.F90:56-57); the full-pencil solver takes the
-                // next cell's (ppm.F90:106-107: cbar = c(i), c(i+1) beside
-                // vxbar(2), vxbar(3) = cells i-1, i)
-                const R cc = PENCIL ? sqrt(gam_ * pp1 / rp1) : sqrt(gam_ * p0 / r0);
-                // characteristic speeds of the cell (order2interp.F90:194-196,221-223)
-                const R lm = (u0 - cc) * rat_, l0 = u0 * rat_, lp = (u0 + cc) * rat_;
-                // x = y/dx of fl/fr (ppm_functs.F90:59-84); the right-side
-                // arguments are exact negations of the left-side ones.
-                const R yp = dt_ * (u0 + cc) * rat_;
-                const R ym = dt_ * (u0 - cc) * rat_;
-                const R y0 = dt_ * u0 * rat_;
-                const R xp = yp / dx_, xm = ym / dx_, x0 = y0 / dx_;
-                const R xtl = (R(0) > yp) ? R(0) / dx_ : xp;          // max(cv,0), atl
-                const R xtr = (R(0) > -ym) ? R(0) / dx_ : -xm;        // max(cv,0), atr
-                // traced values (t: fl/fr at the face; 1,2,3: the -,0,+
-                // characteristics).  All are evaluated, branch-free; the
-                // tracing below selects the ones the reference computes.
-                R ptl, pc1l, pc2l, pc3l, ptr, pc1r, pc2r, pc3r;
-                R rtl, rc2l, rtr, rc2r;
-                R utl, uc1l, uc3l, utr, uc1r, uc3r;
-                R vtl, vc2l, vtr, vc2r, wtl, wc2l, wtr, wc2r;
+                R q1[5], q2[5], q3[5], dm[5], d0[5], dp[5], left[5];
 #pragma unroll
                 for (int q = 0; q < 5; ++q) {
-                    const R q1 = R(S.st[q][ic[1]]), q2 = R(S.st[q][ic[2]]), q3 = R(S.st[q][ic[3]]);
-                    const R dm = S.sl[q][ic[1]], d0 = S.sl[q][ic[2]], dp = S.sl[q][ic[3]];
-                    R Dm = 0, Dp = 0;
-                    const bool st = (q == 1) && steep;
-                    if (q == 1) { Dm = S.d2[ic[1]]; Dp = S.d2[ic[3]]; }
-                    const Parabola<R> Pq = build_parabola<R>(q1, q2, q3, dm, d0, dp, flat, st, Dm, Dp, dx_);
-                    const R tl_ = fl(Pq, xtl), tr_ = fr(Pq, xtr);
-                    if (q == 0) {
-                        ptl = tl_; ptr = tr_;
-                        pc1l = fl(Pq, xm); pc2l = fl(Pq, x0); pc3l = fl(Pq, xp);
-                        pc1r = fr(Pq, -xm); pc2r = fr(Pq, -x0); pc3r = fr(Pq, -xp);
-                    } else if (q == 1) {
-                        rtl = tl_; rtr = tr_;
-                        rc2l = fl(Pq, x0); rc2r = fr(Pq, -x0);
-                    } else if (q == 2) {
-                        utl = tl_; utr = tr_;
-                        uc1l = fl(Pq, xm); uc3l = fl(Pq, xp);
-                        uc1r = fr(Pq, -xm); uc3r = fr(Pq, -xp);
-                    } else if (q == 3) {
-                        vtl = tl_; vtr = tr_;
-                        vc2l = fl(Pq, x0); vc2r = fr(Pq, -x0);
-                    } else {
-                        wtl = tl_; wtr = tr_;
-                        wc2l = fl(Pq, x0); wc2r = fr(Pq, -x0);
-                    }
+                    q1[q] = R(S.st[q][ic[1]]);
+                    q2[q] = R(S.st[q][ic[2]]);
+                    q3[q] = R(S.st[q][ic[3]]);
+                    dm[q] = S.sl[q][ic[1]];
+                    d0[q] = S.sl[q][ic[2]];
+                    dp[q] = S.sl[q][ic[3]];
                 }
-                // negative traced states (order2interp.F90:174-190)
-                if (ptl < R(0)) ptl = R(kTiny);
-                if (ptr < R(0)) ptr = R(kTiny);
-                if (rtl < R(0)) rtl = R(kTiny);
-                if (rtr < R(0)) rtr = R(kTiny);
-                // g at the -/+ characteristics (order2interp.F90:170-172);
-                // gravity off: g == 0
-                R gc1l = R(0), gc3l = R(0), gc1r = R(0), gc3r = R(0);
+                R g1 = R(0), g2 = R(0), g3 = R(0), gdm = R(0), gd0 = R(0), gdp = R(0);
                 if constexpr (GRAV) {
-                    const Parabola<R> Pg = build_parabola<R>(R(S.sg[ic[1]]), R(S.sg[ic[2]]), R(S.sg[ic[3]]),
-                                                             S.slg[ic[1]], S.slg[ic[2]], S.slg[ic[3]], flat, false,
-                                                             R(0), R(0), dx_);
-                    gc1l = fl(Pg, xm);
-                    gc3l = fl(Pg, xp);
-                    gc1r = fr(Pg, -xm);
-                    gc3r = fr(Pg, -xp);
+                    g1 = R(S.sg[ic[1]]); g2 = R(S.sg[ic[2]]); g3 = R(S.sg[ic[3]]);
+                    gdm = S.slg[ic[1]]; gd0 = S.slg[ic[2]]; gdp = S.slg[ic[3]];
                 }
-                // left state of face c+1 (order2interp.F90:192-219,249-258)
-                {
-                    const R ctl = sqrt(gam_ * ptl * rtl);
-                    const R bm_ = beta<R>(ctl, utl, uc1l, ptl, pc1l, gc1l, R(-1), dt_, at_, dat_, rat_);
-                    const R bp_ = beta<R>(ctl, utl, uc3l, ptl, pc3l, gc3l, R(1), dt_, at_, dat_, rat_);
-                    const R b0_ = beta0<R>(ctl, rtl, rc2l, ptl, pc2l, dt_, at_, dat_);
-                    const R bml = (lm > R(0)) ? bm_ : R(0);
-                    const R bpl = (lp > R(0)) ? bp_ : R(0);
-                    const R b0l = (l0 > R(0)) ? b0_ : R(0);
-                    const R vl = (l0 > R(0)) ? vc2l : vtl;
-                    const R wl = (l0 > R(0)) ? wc2l : wtl;
-                    R pl = ptl + ctl * ctl * (bpl + bml);
-                    if (pl <= R(0)) pl = ptl;
-                    const R ul = utl + ctl * (bpl - bml);
-                    R rl = R(1) / (R(1) / rtl - bml - b0l - bpl);
-                    if (rl <= R(0)) rl = rtl;
-                    const int io = ic[2];
-                    S.ls[0][io] = pl;
-                    S.ls[1][io] = rl;
-                    S.ls[2][io] = ul;
-                    S.ls[3][io] = vl;
-                    S.ls[4][io] = wl;
-                }
-                // right state of face c (order2interp.F90:221-258)
-                {
-                    const R ctr = sqrt(gam_ * ptr * rtr);
-                    const R bp_ = beta<R>(ctr, utr, uc3r, ptr, pc3r, gc3r, R(1), dt_, at_, dat_, rat_);
-                    const R bm_ = beta<R>(ctr, utr, uc1r, ptr, pc1r, gc1r, R(-1), dt_, at_, dat_, rat_);
-                    const R b0_ = beta0<R>(ctr, rtr, rc2r, ptr, pc2r, dt_, at_, dat_);
-                    const R bpr = (lp < R(0)) ? bp_ : R(0);
-                    const R bmr = (lm < R(0)) ? bm_ : R(0);
-                    const R b0r = (l0 < R(0)) ? b0_ : R(0);
-                    const R vr = (l0 < R(0)) ? vc2r : vtr;
-                    const R wr = (l0 < R(0)) ? wc2r : wtr;
-                    R pr = ptr + ctr * ctr * (bpr + bmr);
-                    if (pr <= R(0)) pr = ptr;
-                    const R ur = utr + ctr * (bpr - bmr);
-                    R rr = R(1) / (R(1) / rtr - bmr - b0r - bpr);
-                    if (rr <= R(0)) rr = rtr;
-                    right.p = pr;
-                    right.rho = rr;
-                    right.u = ur;
-                    right.v = vr;
-                    right.w = wr;
-                }
+                trace_cell<R, GRAV, PENCIL>(q1, q2, q3, dm, d0, dp, S.d2[ic[1]], S.d2[ic[3]], fl_any, g1, g2, g3, gdm,
+                                            gd0, gdp, ts, left, right);
+                const int io = ic[2];
+#pragma unroll
+                for (int q = 0; q < 5; ++q) S.ls[q][io] = left[q];
             }
         }
         pencil_sync<kWarpStages>();
@@ -681,7 +750,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                                       rho > k.dmax * double(S.st[1][L::idx(d + 1, tp)]);
                     const double cho = (peak && a.cho) ? a.cho[g] : 0.0;
                     integrate_pencil<DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, eel, eer, peak, cho);
-                    finish_cell(g, p, rho, u, v, w);
+                    finish(g, p, rho, u, v, w);
                 }
             }
         } else {
@@ -702,7 +771,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 } else {
                     integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
                 }
-                finish_cell(g, p, rho, u, v, w);
+                finish(g, p, rho, u, v, w);
             }
         }
     }

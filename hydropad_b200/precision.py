@@ -58,7 +58,15 @@ def _sums(test, ref):
 
 
 def _norms_from_sums(s):
-    return {k: {"l1": v[0] / v[1], "linf": v[2] / v[3]} for k, v in s.items()}
+    """Relative norms; a field that is zero everywhere in the reference (the
+    transverse momenta of a plane Sod shock) gets the absolute ones."""
+    out = {}
+    for k, v in s.items():
+        if v[1] > 0.0:
+            out[k] = {"l1": v[0] / v[1], "linf": v[2] / v[3]}
+        else:
+            out[k] = {"l1_abs": v[0], "linf_abs": v[2], "reference": "zero everywhere"}
+    return out
 
 
 def _norms(test, ref):
