@@ -331,7 +331,8 @@ def run_ours(args):
             sm = st.summary()
             serving[prec] = {"p50_s": sm["latency_p50_s"], "p99_s": sm["latency_p99_s"],
                              "value": sm["cell_updates_per_s"], "unit": UNIT, "makespan_s": sm["makespan_s"],
-                             "admission_stalls": sm["admission_stalls"], "tiles": list(stiles),
+                             "admission_stalls": sm["admission_stalls"], "budget_stalls": sm["budget_stalls"],
+                             "peak_resident_gb": sm["peak_resident_gb"], "tiles": list(stiles),
                              # where the host's time went (seconds over the trace)
                              "host_admission_s": sm["host_admission_s"], "host_sync_wait_s": sm["host_sync_wait_s"],
                              "host_retire_s": sm["host_retire_s"], "batch_steps": sm["batch_steps"],

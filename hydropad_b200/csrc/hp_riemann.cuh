@@ -505,13 +505,16 @@ __device__ __forceinline__ void riemann_finish(const FaceState& L, const FaceSta
 // Solve a face whose pattern is known.  RareT is the arithmetic type of the
 // closed two-rarefaction form (double: FP64 path, float: mixed path).  The
 // Eulerian sound speeds (riemannsolver.F90:32-33) are recomputed here, in
-// the type each pattern works in.
-template <class Pow, class RareT, class PowRare>
+// the type each pattern works in.  WHICH restricts the code to the Newton
+// patterns 1, 2 (kNewtonOnly) or the closed forms 3, 4, 5 (kClosedOnly), for
+// a caller that only ever sees those (the same arithmetic, less code).
+enum { kAllPatterns = 0, kNewtonOnly = 1, kClosedOnly = 2 };
+template <class Pow, class RareT, class PowRare, int WHICH = kAllPatterns>
 __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState& L, const FaceState& R,
                                                    FaceState& out, const Consts& k, const StepScalars& s) {
     double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
     bool ok = true;
-    if (pattern == 1 || pattern == 2) {
+    if (WHICH != kClosedOnly && (pattern == 1 || pattern == 2)) {
         double cleft = 0.0, cright = 0.0;
         if (pattern == 2) {
             if constexpr (Pow::kShortNewton) {
@@ -538,7 +541,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
         ok = riemann_newton<Pow>(pm, vxm, L.p, R.p, L.rho, R.rho, L.u, R.u, k);
         if (pattern == 1) sample_two_shocks<RareT>(L, R, pm, vxm, rhom, k);
         else sample_shock_rarefaction<RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
-    } else if (pattern == 3) {
+    } else if (WHICH != kNewtonOnly && pattern == 3) {
         const RareT g = RareT(k.gamma);
         const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);
         const RareT cleft = sqrt(g * pl / rl), cright = sqrt(g * pr / rr);
@@ -563,7 +566,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
                 else riemann_two_rarefactions<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cl, cr, pm, vxm, rhom, k);
             }
         }
-    } else if (pattern == 4) {
+    } else if (WHICH != kNewtonOnly && pattern == 4) {
         const double cleft = sqrt(k.gamma * L.p / L.rho), cright = sqrt(k.gamma * R.p / R.rho);
         riemann_vacuum(L, R, cleft, cright, pm, vxm, rhom, k);
     }

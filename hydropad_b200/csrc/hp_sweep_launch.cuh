@@ -108,9 +108,9 @@ HP_TILE_TABLE(HP_TILE_CHECK)
 // table below, (axis, tile, P, T, NW Newton warps, MINB).
 // ---------------------------------------------------------------------------
 #define HP_WS_TILE_TABLE(X)                                                                   \
-    X(0, 11, 4, 32, 1, 2) X(0, 12, 4, 32, 2, 2) X(0, 13, 8, 32, 2, 1)                         \
-    X(1, 11, 16, 8, 1, 2) X(1, 12, 16, 8, 2, 2) X(1, 13, 16, 16, 2, 1)                        \
-    X(2, 11, 16, 8, 1, 2) X(2, 12, 16, 8, 2, 2) X(2, 13, 16, 16, 2, 1)
+    X(0, 11, 4, 32, 1, 3) X(0, 12, 4, 32, 1, 2) X(0, 13, 8, 32, 1, 1)                         \
+    X(1, 11, 16, 8, 1, 3) X(1, 12, 16, 8, 1, 2) X(1, 13, 16, 16, 1, 1)                        \
+    X(2, 11, 16, 8, 1, 3) X(2, 12, 16, 8, 1, 2) X(2, 13, 16, 16, 1, 1)
 
 // cuTensorMapEncodeTiled of the driver, through the runtime's entry-point
 // query (the library does not link libcuda itself).

@@ -39,6 +39,8 @@
 #pragma once
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "hp_sweep.cuh"
 #include "hp_tma.cuh"
 
@@ -114,6 +116,7 @@ struct WsSmem {
     unsigned short nq[2][3][L::kW];   // Newton faces of a window (by classifying thread), 3 buckets
     unsigned short cq[3][L::kW];      // closed-form faces of the current window
     int nqcnt[2][3];
+    int ntake[2];                     // Newton faces of a window taken so far (chunks of 32)
     int cqcnt[2][3];
     uint64_t full[4];                 // TMA of a ring window complete
     uint64_t nready[2];               // Newton faces of a window queued
@@ -207,6 +210,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
         S.nqcnt[tid / 3][tid % 3] = 0;
         S.cqcnt[tid / 3][tid % 3] = 0;
     }
+    if (tid < 2) S.ntake[tid] = 0;
     __syncthreads();
 
     unsigned long long kmin = kKeyPosInf, kmax = 0ULL, kvel = 0ULL;
@@ -217,8 +221,10 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
     auto item_pencil = [&](int item) { return L::wpencil(item); };
 
     // Riemann problem of face f of pencil tp in window W (pattern known),
-    // density-peak fix, result in place of the right state.
-    auto solve_face = [&](int pattern, int f, int tp, const WsWin& W) {
+    // density-peak fix, result in place of the right state.  `which`: the
+    // patterns this caller sees (the Newton group: 1, 2; the main group's
+    // closed forms: 3, 4, 5), so each role holds only its solver's code.
+    auto solve_face = [&](auto which, int pattern, int f, int tp, const WsWin& W) {
         const int il = L::fi(f - 1, tp, W.ro), io = L::fi(f, tp, W.ro);
         FaceState left, rgt, out;
         left.p = double(S.ls[0][il]);
@@ -231,8 +237,8 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
         rgt.u = S.rs[2][io];
         rgt.v = S.rs[3][io];
         rgt.w = S.rs[4][io];
-        if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare>(pattern, left, rgt, out, k,
-                                                                                         sc))
+        if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare, decltype(which)::value>(
+                pattern, left, rgt, out, k, sc))
             status |= kStatNewton;
         if (peak_possible) {  // riemannsolver.F90:279-285
             double pk;
@@ -254,6 +260,40 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
         S.rs[2][io] = out.u;
         S.rs[3][io] = out.v;
         S.rs[4][io] = out.w;
+    };
+
+    // Solve chunks of 32 Newton faces of window W (queue row k) until the
+    // queue is drained; called by whole warps of either group (the Newton
+    // warps from the window's publication on, the main warps when they reach
+    // the window's update and faces remain).
+    auto drain_newton = [&](int k, const WsWin& W) {
+        const int lane = tid & 31;
+        const int n0 = S.nqcnt[k][0], n1 = S.nqcnt[k][1], n2 = S.nqcnt[k][2];
+        const int total = n0 + n1 + n2;
+        for (;;) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&S.ntake[k], 32);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= total) break;
+            const int i = base + lane;
+            if (i < total) {
+                // the three Newton buckets end to end (shock + rarefaction
+                // on the left, two shocks, shock + rarefaction on the right)
+                int c = 0, idx = i;
+                if (idx >= n0) {
+                    idx -= n0;
+                    c = 1;
+                    if (idx >= n1) {
+                        idx -= n1;
+                        c = 2;
+                    }
+                }
+                const int item = S.nq[k][c][idx];
+                solve_face(std::integral_constant<int, kNewtonOnly>(), pattern_of_bucket(c), item_face(item, W.b),
+                           item_pencil(item), W);
+            }
+        }
+        __syncwarp();
     };
 
     if (tid < L::kMain) {
@@ -438,25 +478,33 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                     // the other row was read by the previous window's closed
                     // forms and is next filled after the next barrier
                     if (tid < 3) S.cqcnt[(s & 1) ^ 1][tid] = 0;
-                    if (pattern) solve_face(pattern, item_face(item, W.b), item_pencil(item), W);
+                    if (pattern)
+                        solve_face(std::integral_constant<int, kClosedOnly>(), pattern, item_face(item, W.b),
+                                   item_pencil(item), W);
                 }
             }
             if (s >= 1) {
                 // ---------------- D: the update of window s-1 ----------------
                 const long long sp = s - 1;
+                // the Newton faces of window s-1 not taken yet, then the
+                // chunks still in the Newton warps
+                drain_newton((int)(sp & 1), ws_window<P, T>(sp, wpg, N));
                 const bool bad = !mbar_wait_bounded(&S.ndone[sp & 1], (uint32_t)((sp >> 1) & 1), &S.abort);
-                // the Newton group has read these counts; they are next
-                // filled by window s+1, after the next barrier
-                if (tid == 0 && !bad) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) S.nqcnt[sp & 1][c] = 0;
-                }
                 if (named_sync_or(1, L::kMain, bad)) {
                     if (tid == 0) {
                         status |= kStatTimeout;
                         S.abort = 1;
                     }
                     break;
+                }
+                // every warp of both groups is done with window s-1's queue
+                // (the Newton warps before ndone, the main warps before the
+                // barrier); its row is next filled by window s+1, after the
+                // next barrier
+                if (tid == 0) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) S.nqcnt[sp & 1][c] = 0;
+                    S.ntake[sp & 1] = 0;
                 }
                 const WsWin W = ws_window<P, T>(s - 1, wpg, N);
                 const bool active = W.pid0 + tp < a.npencil;
@@ -500,7 +548,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
         }
     } else {
         // ======================= Newton group =======================
-        const int wn = (tid - L::kMain) >> 5, lane = tid & 31;
+        const int lane = tid & 31;
         for (long long s = 0; s < nwin; ++s) {
             // every lane waits (acquire of the queue); the warp decides together
             const bool ok = mbar_wait_bounded(&S.nready[s & 1], (uint32_t)((s >> 1) & 1), &S.abort);
@@ -509,25 +557,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                 if (lane == 0) S.abort = 1;
                 break;
             }
-            const WsWin W = ws_window<P, T>(s, wpg, N);
-            const int n0 = S.nqcnt[s & 1][0], n1 = S.nqcnt[s & 1][1], n2 = S.nqcnt[s & 1][2];
-            const int total = n0 + n1 + n2;
-            // the three Newton buckets end to end (shock + rarefaction on the
-            // left, two shocks, shock + rarefaction on the right)
-            for (int i = wn * 32 + lane; i < total; i += NW * 32) {
-                int c = 0, idx = i;
-                if (idx >= n0) {
-                    idx -= n0;
-                    c = 1;
-                    if (idx >= n1) {
-                        idx -= n1;
-                        c = 2;
-                    }
-                }
-                const int item = S.nq[s & 1][c][idx];
-                solve_face(pattern_of_bucket(c), item_face(item, W.b), item_pencil(item), W);
-            }
-            __syncwarp();
+            drain_newton((int)(s & 1), ws_window<P, T>(s, wpg, N));
             if (lane == 0) mbar_arrive(&S.ndone[s & 1]);
         }
     }

@@ -100,6 +100,7 @@ class Member:
 class ServeStats:
     completed: list = field(default_factory=list)
     admission_stalls: int = 0          # step boundaries at which the queue head did not fit
+    budget_stalls: int = 0             # ... of them because of the HBM budget (a free slot, no room)
     stall_seconds: float = 0.0         # summed time the queue head waited for room
     max_queue: int = 0
     peak_resident_bytes: int = 0
@@ -124,6 +125,7 @@ class ServeStats:
             "latency_p99_s": float(np.percentile(lat, 99)),
             "latency_mean_s": float(lat.mean()),
             "admission_stalls": self.admission_stalls,
+            "budget_stalls": self.budget_stalls,
             "admission_stall_s": self.stall_seconds,
             "max_queue": self.max_queue,
             "peak_resident_gb": self.peak_resident_bytes / 1e9,
@@ -142,6 +144,7 @@ def merge_stats(parts) -> ServeStats:
     for st in parts:
         out.completed.extend(st.completed)
         out.admission_stalls += st.admission_stalls
+        out.budget_stalls += st.budget_stalls
         out.stall_seconds += st.stall_seconds
         out.max_queue = max(out.max_queue, st.max_queue)
         out.peak_resident_bytes = max(out.peak_resident_bytes, st.peak_resident_bytes)
@@ -209,6 +212,8 @@ class Scheduler:
                                        resident + box_bytes(queue[0].side) > self.budget)
             if blocked:
                 st.admission_stalls += 1
+                if len(active) < self.capacity:
+                    st.budget_stalls += 1
                 if stall_since is None:
                     stall_since = eng.now()
             elif stall_since is not None:

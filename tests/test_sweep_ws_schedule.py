@@ -176,7 +176,27 @@ def emulate(N, T, groups, seed=0):
     assert not issued, issued
     assert len(updated) == groups * N
     log.check()
+    check_queue_protocol(nwin)
     return log
+
+
+def check_queue_protocol(nwin):
+    """The Newton queue of window s (row s mod 2: counts, chunk counter):
+    filled by C1(s) in (B1(s), B2(s)); drained with atomics by the Newton
+    warps in (B2(s), B3(s+1)) and by the main warps in (B2(s+1), B3(s+1));
+    reset by thread 0 after the barrier B3(s+1) (in (B3(s+1), B1(s+2))).
+    Every drain must end before the reset, and the reset before the next
+    fill of the row (window s+2)."""
+    fill = lambda s: (10 * s, 10 * s + 4)
+    drains = lambda s: [(10 * s + 4, 10 * (s + 1) + 7), (10 * (s + 1) + 4, 10 * (s + 1) + 7)]
+    reset = lambda s: (10 * (s + 1) + 7, 10 * (s + 2))
+    for s in range(nwin):
+        r = reset(s)
+        assert fill(s)[1] <= min(d[0] for d in drains(s))
+        for d in drains(s):
+            assert d[1] <= r[0], ("drain after the reset", s, d, r)
+        if s + 2 < nwin:
+            assert r[1] <= fill(s + 2)[0], ("reset after the next fill", s)
 
 
 # (T) of the compiled pipelined tiles: x T = 32, y/z T = 8 and 16
