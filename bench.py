@@ -370,7 +370,10 @@ def run_ours(args):
         "config": workload_config(n, world, "mixed"),
         "fp64": {"value": fp["value"], "ms_per_step": fp["ms_per_step"], "sweep_ms": fp["sweep_ms"],
                  "tiles": fp["tiles"], "launches": fp["launches"], "clocks": fp["clocks"],
-                 "roofline_frac": BYTES_PER_CELL_SWEEP * cells / (fp["sweep_ms"] * 1e-3) / 1e9 / peaks[0]},
+                 "roofline_frac": BYTES_PER_CELL_SWEEP * cells / (fp["sweep_ms"] * 1e-3) / 1e9 / peaks[0],
+                 # the FP64 sweep's own ceiling: its FP64 pipe's active fraction
+                 # (ncu, profiles/ppm_sweep_fp64_160_ncu_full.md)
+                 "fp64_pipe_frac": load_profile_figure("fp64_pipe_frac")},
         "mixed_over_fp64": mx["value"] / fp["value"],
         "density_rel_l1_mixed_vs_fp64": errs["rho"]["l1"],
         "errors_mixed_vs_fp64": errs,
@@ -400,18 +403,25 @@ def load_peaks():
         return 6650.0, "fallback 6.65 TB/s"
 
 
-def load_traffic(n):
-    """DRAM bytes per sweep launch from the committed ncu summary (captured
-    on a smaller box and scaled by cells), or None."""
+def load_profile_figure(key):
+    """A figure of the committed ncu summary (profiles/ppm_sweep_traffic.txt),
+    or None."""
     path = os.path.join(ROOT, "profiles", "ppm_sweep_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
-                if line.startswith("dram_bytes_per_cell_sweep:"):
-                    return float(line.split(":")[1]) * n ** 3
+                if line.startswith(key + ":"):
+                    return float(line.split(":")[1])
     except OSError:
         pass
     return None
+
+
+def load_traffic(n):
+    """DRAM bytes per sweep launch from the committed ncu summary (captured
+    on a smaller box and scaled by cells), or None."""
+    per_cell = load_profile_figure("dram_bytes_per_cell_sweep")
+    return None if per_cell is None else per_cell * n ** 3
 
 
 # --------------------------------------------------------------------------

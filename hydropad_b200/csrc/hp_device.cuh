@@ -24,6 +24,10 @@ enum : int {
     kFlagResetSpeed = 8,   // zero the velmax accumulator (first sweep of a step)
     kFlagExpandZeroOld = 16,  // expand with vxold = pold3d = 0 (as alloc_arrays.F90:71-74,132-135 leaves them)
     kFlagZHalo = 32,       // z sweep of a slab: the cells beyond its ends come from halo planes
+    // failure-detection test of the pipelined sweep: its Newton warps withhold
+    // the completion of their first window, so that the main group's bounded
+    // wait runs out (set only when HP_TEST_WITHHOLD_NEWTON=1 in the environment)
+    kFlagTestWithhold = 64,
 };
 
 // Time scalars + bookkeeping, one per box, in device memory so that a whole

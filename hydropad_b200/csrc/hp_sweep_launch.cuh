@@ -10,6 +10,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <atomic>
@@ -176,6 +177,10 @@ static int launch_sweep_ws_t(const Box& b, int bslot, int flags, cudaStream_t st
     using L = WsLayout<AXIS, P, T, NW>;
     WsArgs wa;
     memset(&wa, 0, sizeof wa);
+    // the failure-detection test (tests/test_gpu_ws_timeout.py) withholds a
+    // completion so that a bounded wait runs out
+    const char* withhold = getenv("HP_TEST_WITHHOLD_NEWTON");
+    if (withhold && withhold[0] == '1') flags |= kFlagTestWithhold;
     wa.a = make_sweep_args(b, AXIS, bslot, flags);
     if (!make_field_maps<AXIS, P, T>(wa.a, wa.tm)) return -1;
     wa.ngroups = (wa.a.npencil + P - 1) / P;

@@ -558,7 +558,8 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                 break;
             }
             drain_newton((int)(s & 1), ws_window<P, T>(s, wpg, N));
-            if (lane == 0) mbar_arrive(&S.ndone[s & 1]);
+            const bool withhold = s == 0 && (a.flags & kFlagTestWithhold);
+            if (lane == 0 && !withhold) mbar_arrive(&S.ndone[s & 1]);
         }
     }
     block_flush(kmin, kmax, kvel, status, &a.ctl->rho_key[(a.bslot + 1) % 3][0],
