@@ -203,13 +203,13 @@ struct PowF32m {
 // shocks) and 1.01 and 1.1 (shock + rarefaction).  Every start point
 // converges to the same root to the 1e-3 step tolerance; p* differs from
 // the reference's by a few 1e-7 relative at most.
-__device__ __forceinline__ double mixed_newton_start(double pleft, double pright, double rholeft, double rhoright,
-                                                     double vxleft, double vxright, const Consts& k) {
+// FP32 two-rarefaction start value (riemannsolver.F90:118-119), 0 when it
+// is not a positive finite number.
+__device__ __forceinline__ float newton_start_f32(float pl, float pr, float rl, float rr, float ul, float ur,
+                                                  const Consts& k) {
     const float g = float(k.gamma), m = float(k.m);
-    const float pl = float(pleft), pr = float(pright);
-    const float cl = sqrtf(g * pl / float(rholeft)), cr = sqrtf(g * pr / float(rhoright));
-    const float q = (cl + cr + (float(vxleft) - float(vxright)) * (g - 1.0f) * 0.5f) /
-                    (cl / PowF32::pw(pl, m) + cr / PowF32::pw(pr, m));
+    const float cl = sqrtf(g * pl / rl), cr = sqrtf(g * pr / rr);
+    const float q = (cl + cr + (ul - ur) * (g - 1.0f) * 0.5f) / (cl / PowF32::pw(pl, m) + cr / PowF32::pw(pr, m));
     float ps;
     if (k.nroot == 5) {
         const float q2 = q * q;
@@ -217,7 +217,14 @@ __device__ __forceinline__ double mixed_newton_start(double pleft, double pright
     } else {
         ps = PowF32::pw(q, float(k.rm));
     }
-    if (ps > 0.0f && ps < 3.0e38f) return double(ps);
+    return (ps > 0.0f && ps < 3.0e38f) ? ps : 0.0f;
+}
+
+__device__ __forceinline__ double mixed_newton_start(double pleft, double pright, double rholeft, double rhoright,
+                                                     double vxleft, double vxright, const Consts& k) {
+    const float ps = newton_start_f32(float(pleft), float(pright), float(rholeft), float(rhoright), float(vxleft),
+                                      float(vxright), k);
+    if (ps > 0.0f) return double(ps);
     const double kappa = sqrt(k.gamma * (pleft + pright) * (rholeft + rhoright) * 0.25);
     const double pcheck = 0.5 * (pleft + pright) + 0.5 * kappa * (vxleft - vxright);
     return pcheck > 0.0 ? pcheck : 0.0;
@@ -296,6 +303,83 @@ __device__ __forceinline__ bool riemann_newton_short(double& pstar, double& vsta
     }
     vstar = Pow::div_loop((pleft - pright) * ia * ib + vxleft * ib + vxright * ia, ia + ib);
     return ok;
+}
+
+// ------------------------------------------------------------------------
+// Weak Newton faces of the mixed path (patterns 6, 7): the iteration of
+// riemann.F90:60-109 in FP32.
+//
+// A two-shock or shock + rarefaction face is weak when its pressures differ
+// by at most a factor 4 and its velocity jump uL - uR is at most cL + cR
+// (the Eulerian sound speeds of the classification): on the EdS box the
+// star pressure of such faces is then at most 10 times the lower side's
+// (shock Mach number below about 3).  They are 80-99 % of the Newton faces.
+// Strong shocks keep the FP64 iteration, and so does a weak face whose FP32
+// iteration fails (a start value or an iterate that is not a positive
+// finite number, or no convergence within kNewtonMaxF32 steps).
+//
+// The rarefaction wave speed a = m c (1 - x)/(1 - x^m) (x = p*/p of the
+// side, riemann.F90:74-80) has a 0/0 form at x -> 1 that FP32 cannot
+// evaluate as written; with n = 1/m an integer and z = x^(1/n),
+// (1 - x)/(1 - z) = 1 + z + ... + z^(n-1) exactly, so a = m c sum_j z^j,
+// and x^-gf = z/x.  The face states of the mixed path are FP32 values, so
+// the inputs lose nothing in the conversion.
+// ------------------------------------------------------------------------
+constexpr int kNewtonMaxF32 = 20;
+
+__device__ __forceinline__ bool newton_weak(float pl, float pr, float rl, float rr, float ul, float ur, float cl,
+                                            float cr) {
+    const float pmin = fminf(pl, pr), pmax = fmaxf(pl, pr);
+    const float rmin = fminf(rl, rr), rmax = fmaxf(rl, rr);
+    return pmax <= 4.0f * pmin && (ul - ur) <= (cl + cr) && pmin > 1e-18f && pmax < 1e18f && rmin > 1e-18f &&
+           rmax < 1e18f;
+}
+
+// 1/a and the derivative of u* of one side at p* (x = p*/p of the side);
+// sgn = -1 left, +1 right.
+__device__ __forceinline__ void wave_f32(float x, float pstar, float p, float c, float rc, float sgn, int nroot,
+                                         const Consts& k, float& ia, float& vprime) {
+    if (pstar >= p) {  // shock: a = c sqrt(gf x + m)
+        ia = rsqrtf(float(k.gf) * x + float(k.m)) * rc;
+        const float ca = c * ia;
+        vprime = sgn * 0.5f * ia * (1.0f + ca * ca);
+    } else {  // rarefaction: a = m c (1 + z + ... + z^(n-1)), z = x^(1/n)
+        const float z = PowF32::pw(x, float(k.m));
+        float s = 1.0f;
+        for (int j = 1; j < nroot; ++j) s = fmaf(s, z, 1.0f);
+        ia = rc / (float(k.m) * s);
+        vprime = sgn * rc * (z / x);
+    }
+}
+
+__device__ __forceinline__ bool riemann_newton_f32(float& pstar, float& vstar, float pl, float pr, float rl, float rr,
+                                                   float ul, float ur, const Consts& k) {
+    const int n = k.nroot;
+    if (n < 2) return false;
+    const float g = float(k.gamma);
+    const float c2l = g * pl * rl, c2r = g * pr * rr;
+    const float rcl = rsqrtf(c2l), rcr = rsqrtf(c2r);
+    const float cl = c2l * rcl, cr = c2r * rcr;  // Lagrangian sound speeds
+    const float rpl = 1.0f / pl, rpr = 1.0f / pr;
+    const float terr = float(kTerr);
+    float ia = 0.0f, ib = 0.0f;
+    bool ok = false;
+    for (int it = 0; it < kNewtonMaxF32; ++it) {
+        const float old = pstar;
+        float vpl, vpr;
+        wave_f32(pstar * rpl, pstar, pl, cl, rcl, -1.0f, n, k, ia, vpl);
+        wave_f32(pstar * rpr, pstar, pr, cr, rcr, 1.0f, n, k, ib, vpr);
+        const float vsl = ul - (pstar - pl) * ia;
+        const float vsr = ur + (pstar - pr) * ib;
+        pstar = pstar - (vsl - vsr) / (vpl - vpr);
+        if (pstar <= 0.0f) pstar = old * 0.001f;
+        if (!(fabsf(old - pstar) > terr * old)) {
+            ok = true;
+            break;
+        }
+    }
+    vstar = ((pl - pr) * ia * ib + ul * ib + ur * ia) / (ia + ib);
+    return ok && pstar > 0.0f && pstar < 3.0e38f && fabsf(vstar) < 3.0e38f;
 }
 
 template <class Pow>
@@ -502,18 +586,54 @@ __device__ __forceinline__ void riemann_finish(const FaceState& L, const FaceSta
     out.p = pm; out.rho = rhom; out.u = vxm; out.v = vym; out.w = vzm;
 }
 
+// Pattern of a classified face in the mixed path: the weak two-shock and
+// shock + rarefaction faces (newton_weak) become patterns 6 and 7, solved
+// with the FP32 iteration.  The FP64 path keeps patterns 1..5.
+template <bool kWeakNewton>
+__device__ __forceinline__ int solver_pattern(int pattern, float pl, float pr, float rl, float rr, float ul, float ur,
+                                              float cl, float cr) {
+    if constexpr (kWeakNewton) {
+        if ((pattern == 1 || pattern == 2) && newton_weak(pl, pr, rl, rr, ul, ur, cl, cr)) return pattern + 5;
+    }
+    return pattern;
+}
+
 // Solve a face whose pattern is known.  RareT is the arithmetic type of the
 // closed two-rarefaction form (double: FP64 path, float: mixed path).  The
 // Eulerian sound speeds (riemannsolver.F90:32-33) are recomputed here, in
 // the type each pattern works in.  WHICH restricts the code to the Newton
-// patterns 1, 2 (kNewtonOnly) or the closed forms 3, 4, 5 (kClosedOnly), for
-// a caller that only ever sees those (the same arithmetic, less code).
+// patterns 1, 2, 6, 7 (kNewtonOnly) or the closed forms 3, 4, 5
+// (kClosedOnly), for a caller that only ever sees those (the same
+// arithmetic, less code).  Patterns 6 and 7 (mixed path only) are the weak
+// faces of patterns 1 and 2: their p*, u* come from the FP32 iteration, or,
+// if it fails, from the FP64 one as for patterns 1 and 2.
 enum { kAllPatterns = 0, kNewtonOnly = 1, kClosedOnly = 2 };
 template <class Pow, class RareT, class PowRare, int WHICH = kAllPatterns>
 __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState& L, const FaceState& R,
                                                    FaceState& out, const Consts& k, const StepScalars& s) {
     double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
     bool ok = true;
+    if constexpr (Pow::kShortNewton && WHICH != kClosedOnly) {
+        if (pattern == 6 || pattern == 7) {
+            const float pl = float(L.p), pr = float(R.p), rl = float(L.rho), rr = float(R.rho);
+            const float ul = float(L.u), ur = float(R.u);
+            float ps = newton_start_f32(pl, pr, rl, rr, ul, ur, k), us = 0.0f;
+            if (ps > 0.0f && riemann_newton_f32(ps, us, pl, pr, rl, rr, ul, ur, k)) {
+                pm = double(ps);
+                vxm = double(us);
+                if (pattern == 6) {
+                    sample_two_shocks<RareT>(L, R, pm, vxm, rhom, k);
+                } else {
+                    const float g = float(k.gamma);
+                    const double cleft = double(sqrtf(g * pl / rl)), cright = double(sqrtf(g * pr / rr));
+                    sample_shock_rarefaction<RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
+                }
+                riemann_finish(L, R, pm, vxm, rhom, out, s);
+                return true;
+            }
+            pattern -= 5;  // the FP32 iteration failed: FP64 below
+        }
+    }
     if (WHICH != kClosedOnly && (pattern == 1 || pattern == 2)) {
         double cleft = 0.0, cright = 0.0;
         if (pattern == 2) {

@@ -77,6 +77,7 @@ struct PolicyFP64 {
     using RareT = double;      // closed two-rarefaction form
     using PowRare = PowRoot;
     using DivD = DivIEEE;      // divisions of the update
+    static constexpr bool kWeakNewton = false;  // every Newton face in FP64
 };
 // Mixed precision: reconstruction, flattening, characteristic tracing and
 // the traced face states in FP32; the Riemann solver's Newton for p*, u*,
@@ -90,6 +91,7 @@ struct PolicyMixed {
     using RareT = float;         // closed two-rarefaction form: no iteration
     using PowRare = PowRareF32;
     using DivD = PowRootShort;   // update divisions from a refined reciprocal (an ulp or two)
+    static constexpr bool kWeakNewton = true;  // weak Newton faces in FP32 (patterns 6, 7)
 };
 
 template <int AXIS>
@@ -136,16 +138,30 @@ struct SweepLayout {
 
 // Buckets of the Riemann problems, in the order the solving threads take
 // them: shock + rarefaction with the rarefaction on the left (pL >= pR),
-// two shocks, shock + rarefaction with the rarefaction on the right, then
-// the closed forms.  The three Newton buckets share the iteration, and
-// neighbouring buckets differ in the wave on one side only, so a warp that
-// straddles two of them diverges on one side of the loop body.
-constexpr int kBuckets = 6;
-// 1 + bucket of a face of pattern 1..5 (pattern 2: rare_left = pL >= pR)
+// two shocks, shock + rarefaction with the rarefaction on the right (FP64
+// Newton), then, in the mixed path (W), the same three for the weak faces
+// (FP32 Newton, patterns 7, 6, 7), then the closed forms.  The Newton
+// buckets of one precision share the iteration, and neighbouring buckets
+// differ in the wave on one side only, so a warp that straddles two of
+// them diverges on one side of the loop body.
+template <bool W> constexpr int kBucketsOf = W ? 9 : 6;
+// 1 + bucket of a face of pattern 1..7 (patterns 2, 7: rare_left = pL >= pR)
+template <bool W>
 __device__ __forceinline__ int bucket_of(int pattern, bool rare_left) {
-    return pattern == 2 ? (rare_left ? 1 : 3) : (pattern == 1 ? 2 : pattern + 1);
+    if (pattern == 2) return rare_left ? 1 : 3;
+    if (pattern == 1) return 2;
+    if (pattern == 7) return rare_left ? 4 : 6;
+    if (pattern == 6) return 5;
+    return W ? pattern + 4 : pattern + 1;
 }
-__device__ __forceinline__ int pattern_of_bucket(int c) { return (c == 0 || c == 2) ? 2 : (c == 1 ? 1 : c); }
+template <bool W>
+__device__ __forceinline__ int pattern_of_bucket(int c) {
+    if (c == 0 || c == 2) return 2;
+    if (c == 1) return 1;
+    if (W && (c == 3 || c == 5)) return 7;
+    if (W && c == 4) return 6;
+    return W ? c - 3 : c;
+}
 
 template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false, bool PENCIL = false>
 struct SweepSmem {
@@ -153,6 +169,7 @@ struct SweepSmem {
     static constexpr int kC = SweepLayout<AXIS, P, T, RING>::kCells;
     static constexpr int kG = GRAV ? kC : 1;
     static constexpr int kE = PENCIL ? kC : 1;
+    static constexpr int kBuckets = kBucketsOf<Policy::kWeakNewton>;
     double se[kE];              // full-pencil sweeps: new total energy of each cell
     R st[5][kC];                // state ring: p, rho, u, v, w (FP32 copy in the mixed path)
     double sg[kG];              // gravity ring: g = -gforce of this sweep's axis
@@ -458,6 +475,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     constexpr bool kWarpPencils = AXIS == 0 && T <= 32 && (32 % T) == 0;
     constexpr bool kWarpStages = kWarpPencils || L::kYZWarp;  // A -> B -> C1 within a warp
     constexpr bool kDReadsRing = sizeof(R) == sizeof(double) || GRAV;
+    constexpr bool kW = Policy::kWeakNewton;
+    constexpr int kBuckets = kBucketsOf<kW>;
     if (tid < 2 * kBuckets) S.bcnt[tid / kBuckets][tid % kBuckets] = 0;
     __syncthreads();
     int par = 0;  // row of bcnt of this iteration
@@ -619,9 +638,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 const int il = L::idx(f - 1, tpw);
                 CT cl, cr;
                 const CT pl = CT(S.ls[0][il]), pr = CT(right.p);
-                const int pattern = riemann_classify<CT, typename Policy::PowC>(
-                    pl, pr, CT(S.ls[1][il]), CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl, cr, k);
-                bucket = bucket_of(pattern, pl >= pr);
+                const CT rl = CT(S.ls[1][il]), rr = CT(right.rho), ul = CT(S.ls[2][il]), ur = CT(right.u);
+                int pattern = riemann_classify<CT, typename Policy::PowC>(pl, pr, rl, rr, ul, ur, cl, cr, k);
+                pattern = solver_pattern<kW>(pattern, float(pl), float(pr), float(rl), float(rr), float(ul),
+                                             float(ur), float(cl), float(cr));
+                bucket = bucket_of<kW>(pattern, pl >= pr);
             }
             // the lanes of one bucket take a run of its slots with one
             // shared-memory atomic (the order of the runs within a bucket
@@ -644,7 +665,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 const int n = S.bcnt[par][c];
                 if (pattern == 0) {
                     if (idx < n) {
-                        pattern = pattern_of_bucket(c);
+                        pattern = pattern_of_bucket<kW>(c);
                         item = S.work[c][idx];
                     } else {
                         idx -= n;

@@ -288,8 +288,10 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                         c = 2;
                     }
                 }
-                const int item = S.nq[k][c][idx];
-                solve_face(std::integral_constant<int, kNewtonOnly>(), pattern_of_bucket(c), item_face(item, W.b),
+                // bit 15 of the item: a weak face (FP32 Newton, patterns 6, 7)
+                const int item = S.nq[k][c][idx] & 0x7fff;
+                const int pattern = pattern_of_bucket<false>(c) + ((S.nq[k][c][idx] >> 15) ? 5 : 0);
+                solve_face(std::integral_constant<int, kNewtonOnly>(), pattern, item_face(item, W.b),
                            item_pencil(item), W);
             }
         }
@@ -430,6 +432,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                 {
                     const int f = ew - 3;
                     int bucket = 0;  // 1 + bucket of the face, 0: no face
+                    bool weak = false;
                     if (activew && f >= 0 && f <= N) {
                         const int io = L::fi(f, tpw, W.ro);
                         S.rs[0][io] = right.p;
@@ -440,9 +443,15 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                         const int il = L::fi(f - 1, tpw, W.ro);
                         CT cl, cr;
                         const CT pl = CT(S.ls[0][il]), pr = CT(right.p);
-                        const int pattern = riemann_classify<CT, typename Policy::PowC>(
-                            pl, pr, CT(S.ls[1][il]), CT(right.rho), CT(S.ls[2][il]), CT(right.u), cl, cr, k);
-                        bucket = bucket_of(pattern, pl >= pr);
+                        const CT rl = CT(S.ls[1][il]), rr = CT(right.rho), ul = CT(S.ls[2][il]), ur = CT(right.u);
+                        int pattern = riemann_classify<CT, typename Policy::PowC>(pl, pr, rl, rr, ul, ur, cl, cr, k);
+                        pattern = solver_pattern<Policy::kWeakNewton>(pattern, float(pl), float(pr), float(rl),
+                                                                      float(rr), float(ul), float(ur), float(cl),
+                                                                      float(cr));
+                        // the weak faces share the Newton queue rows of
+                        // patterns 1, 2, marked in bit 15 of their item
+                        weak = pattern > 5;
+                        bucket = bucket_of<false>(weak ? pattern - 5 : pattern, pl >= pr);
                     }
                     const int lane = tid & 31;
                     const unsigned peers = __match_any_sync(0xffffffffu, bucket);
@@ -454,7 +463,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                     off = __shfl_sync(0xffffffffu, off, leader);
                     if (bucket) {
                         const int slotq = off + __popc(peers & ((1u << lane) - 1u));
-                        if (bucket <= 3) S.nq[s & 1][bucket - 1][slotq] = (unsigned short)tid;
+                        if (bucket <= 3) S.nq[s & 1][bucket - 1][slotq] = (unsigned short)(tid | (weak ? 0x8000 : 0));
                         else S.cq[bucket - 4][slotq] = (unsigned short)tid;
                     }
                 }
