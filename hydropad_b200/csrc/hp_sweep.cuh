@@ -44,6 +44,8 @@
 #include "hp_physics.cuh"
 #include "hp_riemann.cuh"
 
+#include <type_traits>
+
 namespace hp {
 
 struct SweepArgs {
@@ -78,6 +80,7 @@ struct PolicyFP64 {
     using PowRare = PowRoot;
     using DivD = DivIEEE;      // divisions of the update
     static constexpr bool kWeakNewton = false;  // every Newton face in FP64
+    static constexpr bool kFaceF32 = false;     // face ring in FP64
 };
 // Mixed precision: reconstruction, flattening, characteristic tracing and
 // the traced face states in FP32; the Riemann solver's Newton for p*, u*,
@@ -92,7 +95,23 @@ struct PolicyMixed {
     using PowRare = PowRareF32;
     using DivD = PowRootShort;   // update divisions from a refined reciprocal (an ulp or two)
     static constexpr bool kWeakNewton = true;  // weak Newton faces in FP32 (patterns 6, 7)
+    static constexpr bool kFaceF32 = true;     // face ring in FP32
 };
+
+// Values of the face ring: the traced right state of a face (stage C1),
+// replaced by the face's Riemann state (C2), read by the update (D).  In
+// the mixed path they are FP32: the traced states are FP32 values, and so
+// are the Riemann states except the FP64 Newton's p*, u* of strong shocks
+// and the upwinded transverse velocities (dadt v), which are rounded once.
+// The update forms the fluxes from them in FP64 as integrate.F90 does
+// (products of FP32 values, exact in FP64), so the flux differences of
+// neighbouring faces keep their accuracy in bulk flows.  Forming the fluxes
+// themselves in FP32 (once per face) made the update 4 % cheaper but
+// raised the density L1 against FP64 after 100 steps at 512^3 from 2.8e-6
+// to 1.2e-5: a flux rounded to FP32 in a supersonic bulk flow loses the
+// small difference between neighbouring faces.
+template <class Policy>
+using FaceT = typename std::conditional<Policy::kFaceF32, float, double>::type;
 
 template <int AXIS>
 __device__ __forceinline__ long long pencil_base(long long pid, int nx, int ny) {
@@ -179,9 +198,9 @@ struct SweepSmem {
     unsigned char pf[kC];       // flattening flag of pair (c, c+1)
     R ls[5][kC];                // traced left state (face c+1) from cell c
     // traced right state of face f (from cell f), replaced in place by the
-    // Riemann state of face f: each slot is read and then written by the one
-    // thread that solves that face
-    double rs[5][kC];
+    // Riemann state of face f (FaceT): each slot is read and then written by
+    // the one thread that solves that face
+    FaceT<Policy> rs[5][kC];
     unsigned short work[kBuckets][P * T];  // Riemann problems of the iteration (by the thread
                                            // index that classified them), in buckets
     int bcnt[2][kBuckets];      // bucket fill counts (alternate iterations use alternate rows)
@@ -630,11 +649,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             int bucket = 0;  // 1 + bucket of the face, 0: no face
             if (activew && f >= 0 && f <= N) {
                 const int io = L::idx(f, tpw);
-                S.rs[0][io] = right.p;
-                S.rs[1][io] = right.rho;
-                S.rs[2][io] = right.u;
-                S.rs[3][io] = right.v;
-                S.rs[4][io] = right.w;
+                S.rs[0][io] = FaceT<Policy>(right.p);
+                S.rs[1][io] = FaceT<Policy>(right.rho);
+                S.rs[2][io] = FaceT<Policy>(right.u);
+                S.rs[3][io] = FaceT<Policy>(right.v);
+                S.rs[4][io] = FaceT<Policy>(right.w);
                 const int il = L::idx(f - 1, tpw);
                 CT cl, cr;
                 const CT pl = CT(S.ls[0][il]), pr = CT(right.p);
@@ -725,11 +744,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 }
                 out.p = fmax2(out.p, pk);
             }
-            S.rs[0][io] = out.p;
-            S.rs[1][io] = out.rho;
-            S.rs[2][io] = out.u;
-            S.rs[3][io] = out.v;
-            S.rs[4][io] = out.w;
+            S.rs[0][io] = FaceT<Policy>(out.p);
+            S.rs[1][io] = FaceT<Policy>(out.rho);
+            S.rs[2][io] = FaceT<Policy>(out.u);
+            S.rs[3][io] = FaceT<Policy>(out.v);
+            S.rs[4][io] = FaceT<Policy>(out.w);
         }
         __syncthreads();
         // ---------------- D: cell d = e-4 ----------------

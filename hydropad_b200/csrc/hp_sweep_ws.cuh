@@ -107,7 +107,7 @@ struct WsSmem {
     using R = typename Policy::R;
     using L = WsLayout<AXIS, P, T, NW>;
     double st[5][4 * L::kW];          // state ring (TMA destination), FP64
-    double rs[5][L::kStF];            // right state of a face, then its Riemann solution
+    FaceT<Policy> rs[5][L::kStF];     // right state of a face, then its Riemann solution
     R ls[5][L::kStF];                 // traced left state of face c+1, at the slot of cell c
     R sl[5][L::kStA];                 // ajside slopes
     R d2[L::kStA];                    // dda second difference of rho
@@ -255,11 +255,11 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
             }
             out.p = fmax2(out.p, pk);
         }
-        S.rs[0][io] = out.p;
-        S.rs[1][io] = out.rho;
-        S.rs[2][io] = out.u;
-        S.rs[3][io] = out.v;
-        S.rs[4][io] = out.w;
+        S.rs[0][io] = FaceT<Policy>(out.p);
+        S.rs[1][io] = FaceT<Policy>(out.rho);
+        S.rs[2][io] = FaceT<Policy>(out.u);
+        S.rs[3][io] = FaceT<Policy>(out.v);
+        S.rs[4][io] = FaceT<Policy>(out.w);
     };
 
     // Solve chunks of 32 Newton faces of window W (queue row k) until the
@@ -435,11 +435,11 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                     bool weak = false;
                     if (activew && f >= 0 && f <= N) {
                         const int io = L::fi(f, tpw, W.ro);
-                        S.rs[0][io] = right.p;
-                        S.rs[1][io] = right.rho;
-                        S.rs[2][io] = right.u;
-                        S.rs[3][io] = right.v;
-                        S.rs[4][io] = right.w;
+                        S.rs[0][io] = FaceT<Policy>(right.p);
+                        S.rs[1][io] = FaceT<Policy>(right.rho);
+                        S.rs[2][io] = FaceT<Policy>(right.u);
+                        S.rs[3][io] = FaceT<Policy>(right.v);
+                        S.rs[4][io] = FaceT<Policy>(right.w);
                         const int il = L::fi(f - 1, tpw, W.ro);
                         CT cl, cr;
                         const CT pl = CT(S.ls[0][il]), pr = CT(right.p);
