@@ -418,8 +418,8 @@ def load_profile_figure(key):
 
 
 def load_traffic(n):
-    """DRAM bytes per sweep launch from the committed ncu summary (captured
-    on a smaller box and scaled by cells), or None."""
+    """DRAM bytes per sweep launch from the committed ncu summary (bytes
+    per cell per sweep, times the cells of the box), or None."""
     per_cell = load_profile_figure("dram_bytes_per_cell_sweep")
     return None if per_cell is None else per_cell * n ** 3
 

@@ -291,9 +291,11 @@ int hp_init(const hp_params* p, hp_ctx** out) {
     if (cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(HP_ERR_CUDA);
     for (int q = 0; q < 5; ++q)
         if ((rc = cuda_fail(cudaMalloc(&x->box.f[q], n * sizeof(double)))) != HP_OK) return fail(rc);
+    // expand's step-start snapshot: FP64 in the FP64 path, FP32 in the mixed path
+    const size_t snap_bytes = p->precision == HP_PREC_MIXED ? sizeof(float) : sizeof(double);
     if (p->cosmo && !p->expand_zero_old)
         for (int q = 0; q < 4; ++q)
-            if ((rc = cuda_fail(cudaMalloc(&x->box.snap[q], n * sizeof(double)))) != HP_OK) return fail(rc);
+            if ((rc = cuda_fail(cudaMalloc(&x->box.snap[q], n * snap_bytes))) != HP_OK) return fail(rc);
     // density-peak values of the y/z faces: one per cell (face f < N of a
     // pencil at its cell f) and one per pencil for the last face
     {

@@ -21,7 +21,7 @@ struct TraceRange {
 // One box resident on the device.
 struct Box {
     double* f[5];      // p, rho, vx, vy, vz (natural order), dense (nx,ny,nz), x fastest
-    double* snap[4];   // step-start p, vx, vy, vz (cosmo expand), or null
+    void* snap[4];     // step-start p, vx, vy, vz (cosmo expand): double (FP64 path) or float (mixed), or null
     double* peak;      // density-peak values of the y/z faces (nx*ny*nz + nx*max(ny,nz)), or null
     double* g[3];      // gforce components x, y, z (dense, natural layout), or null: gravity off
     double* zlo;       // slab of a z-split box: 4 halo planes below, [p,rho,vx,vy,vz][4][nx*ny], or null

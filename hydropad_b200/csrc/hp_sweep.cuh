@@ -50,7 +50,7 @@ namespace hp {
 
 struct SweepArgs {
     double* f[5];          // p, rho, u (normal), v, w (transverse) of this sweep
-    double* snap[4];       // step-start p, vx, vy, vz (natural order) for expand
+    void* snap[4];         // step-start p, vx, vy, vz (natural order) for expand, Policy::SnapT
     const double* peak;    // per-face density-peak values for y/z sweeps (may be null)
     const double* g;       // gforce component along this sweep (natural layout), or null: gravity off
     // z sweep of a slab (kFlagZHalo): the 4 planes below and the 3 planes
@@ -79,6 +79,7 @@ struct PolicyFP64 {
     using RareT = double;      // closed two-rarefaction form
     using PowRare = PowRoot;
     using DivD = DivIEEE;      // divisions of the update
+    using SnapT = double;      // step-start snapshot of expand
     static constexpr bool kWeakNewton = false;  // every Newton face in FP64
     static constexpr bool kFaceF32 = false;     // face ring in FP64
 };
@@ -94,6 +95,10 @@ struct PolicyMixed {
     using RareT = float;         // closed two-rarefaction form: no iteration
     using PowRare = PowRareF32;
     using DivD = PowRootShort;   // update divisions from a refined reciprocal (an ulp or two)
+    // expand's step-start snapshot in FP32: it enters the step's end only as
+    // afact * v_old / (2 + afact) and afact * p_old / (1 + afact), with afact
+    // = dt dath / ath a few 1e-2, so its rounding moves v and p by ~1e-9
+    using SnapT = float;
     static constexpr bool kWeakNewton = true;  // weak Newton faces in FP32 (patterns 6, 7)
     static constexpr bool kFaceF32 = true;     // face ring in FP32
 };
@@ -373,17 +378,17 @@ __device__ __forceinline__ void trace_cell(const R q1[5], const R q2[5], const R
 // Stage D's epilogue for cell g (updated state p, rho, u, v, w): expand
 // with the step-start snapshot (expand.F90:18-41), the store, and the
 // step's reductions (rho bounds, speed.F90:25-28 velmax, status).
-template <int AXIS>
+template <int AXIS, class SnapT>
 __device__ __forceinline__ void finish_cell(const SweepArgs& a, long long g, double p, double rho, double u, double v,
                                             double w, double afact, double afact1, double afact2,
                                             unsigned long long& kmin, unsigned long long& kmax,
                                             unsigned long long& kvel, unsigned& status) {
     if (a.flags & kFlagExpand) {
         const bool zero_old = (a.flags & kFlagExpandZeroOld) != 0;
-        const double vx_o = zero_old ? 0.0 : a.snap[1][g];
-        const double vy_o = zero_old ? 0.0 : a.snap[2][g];
-        const double vz_o = zero_old ? 0.0 : a.snap[3][g];
-        const double p_o = zero_old ? 0.0 : a.snap[0][g];
+        const double vx_o = zero_old ? 0.0 : double(static_cast<const SnapT*>(a.snap[1])[g]);
+        const double vy_o = zero_old ? 0.0 : double(static_cast<const SnapT*>(a.snap[2])[g]);
+        const double vz_o = zero_old ? 0.0 : double(static_cast<const SnapT*>(a.snap[3])[g]);
+        const double p_o = zero_old ? 0.0 : double(static_cast<const SnapT*>(a.snap[0])[g]);
         const double un_o = AXIS == 0 ? vx_o : (AXIS == 1 ? vy_o : vz_o);
         const double v_o = AXIS == 0 ? vy_o : (AXIS == 1 ? vx_o : vy_o);
         const double w_o = AXIS == 0 ? vz_o : (AXIS == 1 ? vz_o : vx_o);
@@ -528,7 +533,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     };
     // D's epilogue: expand, store, and the step's reductions
     auto finish = [&](long long g, double p, double rho, double u, double v, double w) {
-        finish_cell<AXIS>(a, g, p, rho, u, v, w, afact, afact1, afact2, kmin, kmax, kvel, status);
+        finish_cell<AXIS, typename Policy::SnapT>(a, g, p, rho, u, v, w, afact, afact1, afact2, kmin, kmax, kvel,
+                                                  status);
     };
 
     for (int b = -4; b <= N + 3 + kLag; b += T, par ^= 1) {
@@ -568,10 +574,11 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                     double vx = AXIS == 0 ? v[2] : (AXIS == 1 ? v[3] : v[4]);
                     double vy = AXIS == 0 ? v[3] : (AXIS == 1 ? v[2] : v[3]);
                     double vz = AXIS == 0 ? v[4] : (AXIS == 1 ? v[4] : v[2]);
-                    a.snap[0][g] = v[0];
-                    a.snap[1][g] = vx;
-                    a.snap[2][g] = vy;
-                    a.snap[3][g] = vz;
+                    using SnapT = typename Policy::SnapT;
+                    static_cast<SnapT*>(a.snap[0])[g] = SnapT(v[0]);
+                    static_cast<SnapT*>(a.snap[1])[g] = SnapT(vx);
+                    static_cast<SnapT*>(a.snap[2])[g] = SnapT(vy);
+                    static_cast<SnapT*>(a.snap[3])[g] = SnapT(vz);
                 }
             }
             const int ix = L::idx(e, tp);

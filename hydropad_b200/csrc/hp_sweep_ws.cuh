@@ -530,10 +530,11 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                     double p = S.st[0][ic], rho = S.st[1][ic], u = S.st[2][ic], v = S.st[3][ic], w = S.st[4][ic];
                     if (a.flags & kFlagSnapshot) {
                         // the step-start state, natural order p, vx, vy, vz
-                        a.snap[0][g] = p;
-                        a.snap[1][g] = AXIS == 0 ? u : (AXIS == 1 ? v : w);
-                        a.snap[2][g] = AXIS == 0 ? v : (AXIS == 1 ? u : v);
-                        a.snap[3][g] = AXIS == 0 ? w : (AXIS == 1 ? w : u);
+                        using SnapT = typename Policy::SnapT;
+                        static_cast<SnapT*>(a.snap[0])[g] = SnapT(p);
+                        static_cast<SnapT*>(a.snap[1])[g] = SnapT(AXIS == 0 ? u : (AXIS == 1 ? v : w));
+                        static_cast<SnapT*>(a.snap[2])[g] = SnapT(AXIS == 0 ? v : (AXIS == 1 ? u : v));
+                        static_cast<SnapT*>(a.snap[3])[g] = SnapT(AXIS == 0 ? w : (AXIS == 1 ? w : u));
                     }
                     // total() with the natural component order (ppmsolver.F90:149,277,405)
                     double etot;
@@ -541,7 +542,8 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                     else etot = total_energy(p, rho, u, v, w, k.rgamma1);
                     const double eint = p * k.rgamma1;
                     integrate<false, DivD>(f1, f2, p, rho, u, v, w, etot, eint, k, sc, 0.0);
-                    finish_cell<AXIS>(a, g, p, rho, u, v, w, afact, afact1, afact2, kmin, kmax, kvel, status);
+                    finish_cell<AXIS, typename Policy::SnapT>(a, g, p, rho, u, v, w, afact, afact1, afact2, kmin, kmax, kvel,
+                                                              status);
                 }
             }
         }

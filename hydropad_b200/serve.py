@@ -36,14 +36,15 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-# device bytes per cell of one box: 5 state fields, 4 snapshot fields
-# (expand), 1 density-peak buffer, all FP64
-BYTES_PER_CELL = 10 * 8
+# device bytes per cell of one box: 5 FP64 state fields, 1 FP64
+# density-peak buffer and the 4 fields of expand's step-start snapshot
+# (FP64 in the FP64 path, FP32 in the mixed path)
+BYTES_PER_CELL = {"fp64": 10 * 8, "mixed": 6 * 8 + 4 * 4}
 CTL_BYTES = 4096
 
 
-def box_bytes(side: int) -> int:
-    return BYTES_PER_CELL * side ** 3 + CTL_BYTES
+def box_bytes(side: int, precision: str = "fp64") -> int:
+    return BYTES_PER_CELL[precision] * side ** 3 + CTL_BYTES
 
 
 @dataclass
@@ -173,6 +174,7 @@ class Scheduler:
 
     def __init__(self, engine, budget_bytes: int, capacity: int = 64, chunk: int = 8, keep_results: bool = False):
         self.engine = engine
+        self.precision = getattr(engine, "precision", "fp64")
         self.budget = int(budget_bytes)
         self.capacity = int(capacity)
         self.chunk = max(1, int(chunk))
@@ -188,7 +190,7 @@ class Scheduler:
         stall_since = None
         inflight = False  # a chunk of the current members is enqueued and not yet accounted
         for r in pending:
-            if box_bytes(r.side) > self.budget:
+            if box_bytes(r.side, self.precision) > self.budget:
                 raise ValueError(f"request {r.rid} (side {r.side}) can never fit the HBM budget")
         while pending or queue or active:
             now = eng.now()
@@ -197,7 +199,7 @@ class Scheduler:
             st.max_queue = max(st.max_queue, len(queue))
             # admission, FIFO: the head blocks the rest
             while queue and len(active) < self.capacity:
-                need = box_bytes(queue[0].side)
+                need = box_bytes(queue[0].side, self.precision)
                 if resident + need > self.budget:
                     break
                 req = queue.popleft()
@@ -209,7 +211,7 @@ class Scheduler:
                 active.append(Member(req, box, req.steps, eng.now()))
             st.peak_resident_bytes = max(st.peak_resident_bytes, resident)
             blocked = bool(queue) and (len(active) >= self.capacity or
-                                       resident + box_bytes(queue[0].side) > self.budget)
+                                       resident + box_bytes(queue[0].side, self.precision) > self.budget)
             if blocked:
                 st.admission_stalls += 1
                 if len(active) < self.capacity:
@@ -246,7 +248,7 @@ class Scheduler:
                     st.completed.append(Completed(m.req.rid, m.req.side, m.req.steps, m.req.arrival, m.admitted, t,
                                                   res if self.keep_results else None))
                     eng.release(m.box)
-                    resident -= box_bytes(m.req.side)
+                    resident -= box_bytes(m.req.side, self.precision)
         if stall_since is not None:
             st.stall_seconds += eng.now() - stall_since
         st.wall = eng.now()
@@ -307,7 +309,7 @@ class GpuEngine:
         free = self.pool.get(req.side)
         if free:
             h = free.pop()
-            self.pooled -= box_bytes(req.side)
+            self.pooled -= box_bytes(req.side, self.precision)
             self.reused += 1
             h.set_scalars(self.initial[req.side])
         else:
@@ -340,9 +342,9 @@ class GpuEngine:
 
     def release(self, h):
         side = int(h.params.shape[0])
-        if self.pooled + box_bytes(side) <= self.pool_bytes:
+        if self.pooled + box_bytes(side, self.precision) <= self.pool_bytes:
             self.pool.setdefault(side, []).append(h)
-            self.pooled += box_bytes(side)
+            self.pooled += box_bytes(side, self.precision)
         else:
             h.close()
 

@@ -18,10 +18,12 @@ def test_serving_matches_alone(precision, pool):
     from hydropad_b200.serve import GpuEngine, Request, Scheduler, box_bytes, run_alone
     reqs = [Request(0, 0.0, 32, 14, 101), Request(1, 0.0, 48, 9, 102), Request(2, 0.0, 32, 21, 103),
             Request(3, 0.0, 16 * 3, 6, 104), Request(4, 0.0, 32, 11, 105)]
-    eng = GpuEngine(precision, capacity=3, tiles=TILES, graph=True, pool_bytes=10 * box_bytes(48) if pool else 0)
+    eng = GpuEngine(precision, capacity=3, tiles=TILES, graph=True,
+                    pool_bytes=10 * box_bytes(48, precision) if pool else 0)
     try:
         # room for about two boxes: later requests wait and join mid-run
-        sched = Scheduler(eng, budget_bytes=box_bytes(48) + box_bytes(32), capacity=3, chunk=4, keep_results=True)
+        sched = Scheduler(eng, budget_bytes=box_bytes(48, precision) + box_bytes(32, precision), capacity=3,
+                          chunk=4, keep_results=True)
         eng.start_clock()
         st = sched.run(reqs)
         reused = eng.reused
