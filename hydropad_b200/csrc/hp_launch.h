@@ -48,9 +48,9 @@ int launch_timedet(const Box& b, int advance, cudaStream_t st);
 constexpr int kNumClassicTiles = 11;
 constexpr int kNumWsTiles = 3;
 constexpr int kNumTiles = kNumClassicTiles + kNumWsTiles;
-constexpr int kTilePencils[3][kNumClassicTiles] = {{8, 4, 8, 4, 16, 12, 8, 16, 8, 8, 16},
-                                            {32, 16, 32, 16, 64, 32, 32, 32, 32, 16, 16},
-                                            {32, 16, 32, 16, 64, 32, 32, 32, 32, 16, 16}};
+constexpr int kTilePencils[3][kNumClassicTiles] = {{8, 4, 8, 4, 16, 12, 8, 16, 16, 8, 16},
+                                            {32, 16, 32, 16, 64, 32, 32, 32, 64, 16, 16},
+                                            {32, 16, 32, 16, 64, 32, 32, 32, 64, 16, 16}};
 
 struct BatchLaunch;  // hp_sweep.cuh
 

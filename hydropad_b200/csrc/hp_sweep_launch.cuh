@@ -91,13 +91,13 @@ static int launch_sweep_t(const Box& b, int bslot, int flags, cudaStream_t st) {
 #define HP_TILE_TABLE(X)                                                                       \
     X(0, 0, 8, 32, 64, 1) X(0, 1, 4, 32, 64, 1) X(0, 2, 8, 16, 32, 1) X(0, 3, 4, 16, 32, 1)    \
     X(0, 4, 16, 32, 64, 1) X(0, 5, 12, 32, 64, 1) X(0, 6, 8, 32, 64, 3) X(0, 7, 16, 16, 32, 4)  \
-    X(0, 8, 8, 32, 64, 2) X(0, 9, 8, 32, 64, 4) X(0, 10, 16, 16, 32, 3)                        \
+    X(0, 8, 16, 32, 64, 2) X(0, 9, 8, 32, 64, 4) X(0, 10, 16, 16, 32, 3)                        \
     X(1, 0, 32, 8, 16, 1) X(1, 1, 16, 8, 16, 1) X(1, 2, 32, 4, 16, 1) X(1, 3, 16, 4, 16, 1)    \
     X(1, 4, 64, 8, 16, 1) X(1, 5, 32, 12, 32, 1) X(1, 6, 32, 8, 16, 3) X(1, 7, 32, 8, 16, 4)   \
-    X(1, 8, 32, 8, 16, 2) X(1, 9, 16, 16, 32, 4) X(1, 10, 16, 16, 32, 3)                         \
+    X(1, 8, 64, 8, 16, 2) X(1, 9, 16, 16, 32, 4) X(1, 10, 16, 16, 32, 3)                         \
     X(2, 0, 32, 8, 16, 1) X(2, 1, 16, 8, 16, 1) X(2, 2, 32, 4, 16, 1) X(2, 3, 16, 4, 16, 1)    \
     X(2, 4, 64, 8, 16, 1) X(2, 5, 32, 12, 32, 1) X(2, 6, 32, 8, 16, 3) X(2, 7, 32, 8, 16, 4)   \
-    X(2, 8, 32, 8, 16, 2) X(2, 9, 16, 16, 32, 4) X(2, 10, 16, 16, 32, 3)
+    X(2, 8, 64, 8, 16, 2) X(2, 9, 16, 16, 32, 4) X(2, 10, 16, 16, 32, 3)
 
 #define HP_TILE_CHECK(AX, TI, P, T, RING, MINB) \
     static_assert(kTilePencils[AX][TI] == P, "tile table and kTilePencils disagree");
