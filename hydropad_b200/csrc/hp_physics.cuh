@@ -187,6 +187,10 @@ __device__ __forceinline__ R beta0(R ct, R rhot, R rhoc, R pt, R pc, R dt, R at,
 struct FaceState {
     double p, rho, u, v, w;
 };
+// The face state of the mixed path's FP32 solvers.
+struct FaceF {
+    float p, rho, u, v, w;
+};
 
 // Density-peak pressure fix, riemannsolver.F90:279-285.  r1..r4 / u2,u3 are
 // rhobar(1..4) / vxbar(2..3) of the gather (cells f-3..f of the sweep).

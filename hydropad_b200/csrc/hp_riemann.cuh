@@ -418,10 +418,11 @@ __device__ __forceinline__ double start_two_shocks(const FaceState& L, const Fac
 }
 
 // Sampling of pattern 1 after the Newton solve, riemannsolver.F90:82-109.
-template <class S>
-__device__ __forceinline__ void sample_two_shocks(const FaceState& L, const FaceState& R, double& pm, double& vxm,
-                                                  double& rhom, const Consts& k) {
-    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
+// S: the arithmetic type; FS / O: the face-state and result types (FaceState
+// and double, or the mixed path's FP32 FaceF and float).
+template <class S, class FS = FaceState, class O = double>
+__device__ __forceinline__ void sample_two_shocks(const FS& L, const FS& R, O& pm, O& vxm, O& rhom, const Consts& k) {
+    const auto pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
     const S pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
     const S rl = S(rholeft), rr = S(rhoright);
     const S rhoshock1 = rhoshock<S>(pmS, S(pleft), rl, g1);
@@ -432,8 +433,8 @@ __device__ __forceinline__ void sample_two_shocks(const FaceState& L, const Face
     if (rhoshock2 == rr) vshock2 = S(0);
     else vshock2 = (rhoshock2 * vxmS - rr * S(vxright)) / (rhoshock2 - rr);
     if (vshock2 < S(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
-    else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = double(rhoshock2);
-    else if (vshock1 <= S(0) && vxm > 0.0) rhom = double(rhoshock1);
+    else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = O(rhoshock2);
+    else if (vshock1 <= S(0) && vxm > 0.0) rhom = O(rhoshock1);
     else { pm = pleft; vxm = vxleft; rhom = rholeft; }
 }
 
@@ -454,12 +455,11 @@ __device__ __forceinline__ double start_shock_rarefaction(const FaceState& L, co
 
 // Sampling of pattern 2 after the Newton solve, riemannsolver.F90:124-184,
 // with the powers of PowS.
-template <class S, class PowS>
-__device__ __forceinline__ void sample_shock_rarefaction(const FaceState& L, const FaceState& R, double cleft,
-                                                         double cright, double& pm, double& vxm, double& rhom,
-                                                         const Consts& k) {
+template <class S, class PowS, class FS = FaceState, class O = double>
+__device__ __forceinline__ void sample_shock_rarefaction(const FS& L, const FS& R, O cleft, O cright, O& pm, O& vxm,
+                                                         O& rhom, const Consts& k) {
     const double gamma = k.gamma;
-    const double pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
+    const auto pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
     const S gS = S(gamma), pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
     if (pleft >= pright) {
         const S rr = S(rhoright), rl = S(rholeft);
@@ -472,12 +472,12 @@ __device__ __forceinline__ void sample_shock_rarefaction(const FaceState& L, con
         const S vhead1 = S(vxleft) - S(cleft);
         if (vshock2 < S(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
         else if (vhead1 >= S(0)) { pm = pleft; vxm = vxleft; rhom = rholeft; }
-        else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = double(rhoshock2);
-        else if (vxm > 0.0 && vtail1 <= S(0)) rhom = double(rhocont1);
+        else if (vxm <= 0.0 && vshock2 >= S(0)) rhom = O(rhoshock2);
+        else if (vxm > 0.0 && vtail1 <= S(0)) rhom = O(rhocont1);
         else if (vtail1 > S(0) && vhead1 <= S(0)) {
-            pm = double(rarwave<S>(S(pleft), pmS, vtail1, vhead1));
-            rhom = double(rarwave<S>(rl, rhocont1, vtail1, vhead1));
-            vxm = double(rarwave<S>(S(vxleft), vxmS, vtail1, vhead1));
+            pm = O(rarwave<S>(S(pleft), pmS, vtail1, vhead1));
+            rhom = O(rarwave<S>(rl, rhocont1, vtail1, vhead1));
+            vxm = O(rarwave<S>(S(vxleft), vxmS, vtail1, vhead1));
         }
     } else {
         const S rr = S(rhoright), rl = S(rholeft);
@@ -490,12 +490,12 @@ __device__ __forceinline__ void sample_shock_rarefaction(const FaceState& L, con
         const S vhead2 = S(vxright) + S(cright);
         if (vshock1 > S(0)) { pm = pleft; vxm = vxleft; rhom = rholeft; }
         else if (vhead2 <= S(0)) { pm = pright; vxm = vxright; rhom = rhoright; }
-        else if (vxm >= 0.0 && vshock1 <= S(0)) rhom = double(rhoshock1);
-        else if (vxm < 0.0 && vtail2 >= S(0)) rhom = double(rhocont2);
+        else if (vxm >= 0.0 && vshock1 <= S(0)) rhom = O(rhoshock1);
+        else if (vxm < 0.0 && vtail2 >= S(0)) rhom = O(rhocont2);
         else if (vtail2 < S(0) && vhead2 >= S(0)) {
-            pm = double(rarwave<S>(S(pright), pmS, vtail2, vhead2));
-            rhom = double(rarwave<S>(rr, rhocont2, vtail2, vhead2));
-            vxm = double(rarwave<S>(S(vxright), vxmS, vtail2, vhead2));
+            pm = O(rarwave<S>(S(pright), pmS, vtail2, vhead2));
+            rhom = O(rarwave<S>(rr, rhocont2, vtail2, vhead2));
+            vxm = O(rarwave<S>(S(vxright), vxmS, vtail2, vhead2));
         }
     }
 }
@@ -692,6 +692,54 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
     }
     riemann_finish(L, R, pm, vxm, rhom, out, s);
     return ok;
+}
+
+// The mixed path's FP32 faces on FP32 states: the two-rarefaction closed
+// form (pattern 3) and the FP32 Newton of weak faces (patterns 6, 7), the
+// same arithmetic as riemann_by_pattern's FP32 branches without widening
+// the face states to FP64 and back (the face rings of the mixed path hold
+// FP32 values).
+// Returns false, with out unset, for every other pattern and for a face
+// whose FP32 solution fails (a non-positive or NaN star state, an FP32
+// iteration that does not converge); riemann_by_pattern then solves it in
+// FP64 (pattern 3, or 1 / 2 for a failed 6 / 7).  The transverse factor
+// dadt = 1 - eps (riemannsolver.F90:36, eps = dat dt rat / 2 a few 1e-3)
+// enters as v - eps v with eps in FP32: an FP32 dadt would carry its own
+// rounding (up to 6e-8 relative) into every transverse flux of every sweep
+// with the same sign, while eps v rounds at 1e-10 of v.
+__device__ __forceinline__ bool riemann_mixed_f32(int pattern, const FaceF& L, const FaceF& R, FaceF& out,
+                                                  const Consts& k, float eps) {
+    float pm, vxm, rhom;
+    const float g = float(k.gamma);
+    if (pattern == 3) {
+        const float cleft = sqrtf(g * L.p / L.rho), cright = sqrtf(g * R.p / R.rho);
+        pm = vxm = rhom = __int_as_float(0x7fc00000);
+        riemann_two_rarefactions<float, PowRareF32>(L.p, R.p, L.rho, R.rho, L.u, R.u, cleft, cright, pm, vxm, rhom,
+                                                    k);
+        if (!(pm > 0.0f && rhom > 0.0f && vxm == vxm)) return false;
+    } else if (pattern == 6 || pattern == 7) {
+        float ps = newton_start_f32(L.p, R.p, L.rho, R.rho, L.u, R.u, k), us = 0.0f;
+        if (!(ps > 0.0f && riemann_newton_f32(ps, us, L.p, R.p, L.rho, R.rho, L.u, R.u, k))) return false;
+        pm = ps;
+        vxm = us;
+        rhom = __int_as_float(0x7fc00000);
+        if (pattern == 6) {
+            sample_two_shocks<float>(L, R, pm, vxm, rhom, k);
+        } else {
+            const float cleft = sqrtf(g * L.p / L.rho), cright = sqrtf(g * R.p / R.rho);
+            sample_shock_rarefaction<float, PowRareF32>(L, R, cleft, cright, pm, vxm, rhom, k);
+        }
+    } else {
+        return false;
+    }
+    // transverse velocities upwinded by the sign of u* (riemannsolver.F90:269-275)
+    out.p = pm;
+    out.rho = rhom;
+    out.u = vxm;
+    const float vt = vxm >= 0.0f ? L.v : R.v, wt = vxm >= 0.0f ? L.w : R.w;
+    out.v = fmaf(-eps, vt, vt);
+    out.w = fmaf(-eps, wt, wt);
+    return true;
 }
 
 // riemannsolver, riemannsolver.F90:1-285, for a single face in FP64 (the

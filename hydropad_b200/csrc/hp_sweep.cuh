@@ -474,6 +474,9 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
         if (a.flags & kFlagResetSpeed) a.ctl->velmax_key = 0ULL;
     }
 
+    // the transverse factor dadt = 1 - dadt_eps of riemann_finish
+    // (riemannsolver.F90:36) for the mixed path's FP32 faces
+    const float dadt_eps = float(0.5 * sc.dat * sc.dt * sc.rat);
     // expand.F90:18-20
     const double afact = sc.dt * (sc.dath / sc.ath);
     const double afact1 = 1.0 / (1.0 + afact);
@@ -707,55 +710,76 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             const int wtp = L::wpencil(item);
             const int f = b - 3 + L::wcell(item);
             const int il = L::idx(f - 1, wtp), io = L::idx(f, wtp);
-            FaceState left, rgt, out;
-            left.p = double(S.ls[0][il]);
-            left.rho = double(S.ls[1][il]);
-            left.u = double(S.ls[2][il]);
-            left.v = double(S.ls[3][il]);
-            left.w = double(S.ls[4][il]);
-            rgt.p = S.rs[0][io];
-            rgt.rho = S.rs[1][io];
-            rgt.u = S.rs[2][io];
-            rgt.v = S.rs[3][io];
-            rgt.w = S.rs[4][io];
-            if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare>(
-                    pattern, left, rgt, out, k, sc))
-                status |= kStatNewton;
-            // density-peak fix (riemannsolver.F90:279-285)
-            if (AXIS == 2 && (a.flags & kFlagZHalo) && peak_possible) {
-                // the transposed gather of the z peak test reaches across
-                // slabs; a slab reports it instead of applying it
-                status |= kStatUnsupported;
-            } else if (peak_possible) {
-                double pk;
+            // density-peak fix (riemannsolver.F90:279-285): the pressure
+            // floor of face f, -inf when the fix does not apply
+            auto peak_floor = [&]() -> double {
+                if (AXIS == 2 && (a.flags & kFlagZHalo)) {
+                    // the transposed gather of the z peak test reaches
+                    // across slabs; a slab reports it instead of applying it
+                    status |= kStatUnsupported;
+                    return -__longlong_as_double(0x7ff0000000000000ULL);
+                }
                 if constexpr (PENCIL) {
                     // the full-pencil solver's 5-cell window along the sweep:
                     // rhobar(1..4) = cells f-2..f+1, vxbar(2..3) = f-1, f
-                    pk = peak_value(S.st[1][L::idx(f - 2, wtp)], S.st[1][L::idx(f - 1, wtp)],
-                                    S.st[1][L::idx(f, wtp)], S.st[1][L::idx(f + 1, wtp)],
-                                    S.st[2][L::idx(f - 1, wtp)], S.st[2][L::idx(f, wtp)], k.dmax);
+                    return peak_value(S.st[1][L::idx(f - 2, wtp)], S.st[1][L::idx(f - 1, wtp)],
+                                      S.st[1][L::idx(f, wtp)], S.st[1][L::idx(f + 1, wtp)],
+                                      S.st[2][L::idx(f - 1, wtp)], S.st[2][L::idx(f, wtp)], k.dmax);
                 } else if (AXIS == 0) {
-                    pk = peak_value(S.st[1][L::idx(f - 3, wtp)], S.st[1][L::idx(f - 2, wtp)],
-                                    S.st[1][L::idx(f - 1, wtp)], S.st[1][L::idx(f, wtp)],
-                                    S.st[2][L::idx(f - 2, wtp)], S.st[2][L::idx(f - 1, wtp)], k.dmax);
+                    return peak_value(S.st[1][L::idx(f - 3, wtp)], S.st[1][L::idx(f - 2, wtp)],
+                                      S.st[1][L::idx(f - 1, wtp)], S.st[1][L::idx(f, wtp)],
+                                      S.st[2][L::idx(f - 2, wtp)], S.st[2][L::idx(f - 1, wtp)], k.dmax);
                 } else {
                     // the reference gathers these with the x index slot
                     // (ppmsolver.F90:251-252, 379-380); a pre-pass has
                     // evaluated them on the pre-sweep state: face f < N at
                     // the index of cell f, face N after the last cell
-                    if (f < N) {
-                        pk = a.peak[pencil_base<AXIS>(pid0 + wtp, a.nx, a.ny) + stride * f];
-                    } else {
-                        pk = a.peak[(long long)a.nx * a.ny * a.nz + pid0 + wtp];
-                    }
+                    if (f < N) return a.peak[pencil_base<AXIS>(pid0 + wtp, a.nx, a.ny) + stride * f];
+                    return a.peak[(long long)a.nx * a.ny * a.nz + pid0 + wtp];
                 }
-                out.p = fmax2(out.p, pk);
+            };
+            bool solved = false;
+            if constexpr (Policy::kFaceF32) {
+                // the mixed path's FP32 faces straight from the FP32 rings
+                FaceF lf, rf, of;
+                lf.p = S.ls[0][il]; lf.rho = S.ls[1][il]; lf.u = S.ls[2][il]; lf.v = S.ls[3][il];
+                lf.w = S.ls[4][il];
+                rf.p = S.rs[0][io]; rf.rho = S.rs[1][io]; rf.u = S.rs[2][io]; rf.v = S.rs[3][io];
+                rf.w = S.rs[4][io];
+                if (riemann_mixed_f32(pattern, lf, rf, of, k, dadt_eps)) {
+                    if (peak_possible) of.p = float(fmax2(double(of.p), peak_floor()));
+                    S.rs[0][io] = of.p;
+                    S.rs[1][io] = of.rho;
+                    S.rs[2][io] = of.u;
+                    S.rs[3][io] = of.v;
+                    S.rs[4][io] = of.w;
+                    solved = true;
+                } else if (pattern >= 6) {
+                    pattern -= 5;  // the FP32 iteration failed: FP64
+                }
             }
-            S.rs[0][io] = FaceT<Policy>(out.p);
-            S.rs[1][io] = FaceT<Policy>(out.rho);
-            S.rs[2][io] = FaceT<Policy>(out.u);
-            S.rs[3][io] = FaceT<Policy>(out.v);
-            S.rs[4][io] = FaceT<Policy>(out.w);
+            if (!solved) {
+                FaceState left, rgt, out;
+                left.p = double(S.ls[0][il]);
+                left.rho = double(S.ls[1][il]);
+                left.u = double(S.ls[2][il]);
+                left.v = double(S.ls[3][il]);
+                left.w = double(S.ls[4][il]);
+                rgt.p = S.rs[0][io];
+                rgt.rho = S.rs[1][io];
+                rgt.u = S.rs[2][io];
+                rgt.v = S.rs[3][io];
+                rgt.w = S.rs[4][io];
+                if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare>(
+                        pattern, left, rgt, out, k, sc))
+                    status |= kStatNewton;
+                if (peak_possible) out.p = fmax2(out.p, peak_floor());
+                S.rs[0][io] = FaceT<Policy>(out.p);
+                S.rs[1][io] = FaceT<Policy>(out.rho);
+                S.rs[2][io] = FaceT<Policy>(out.u);
+                S.rs[3][io] = FaceT<Policy>(out.v);
+                S.rs[4][io] = FaceT<Policy>(out.w);
+            }
         }
         __syncthreads();
         // ---------------- D: cell d = e-4 ----------------

@@ -181,6 +181,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
     const long long stride = axis_stride<AXIS>(a.nx, a.ny);
     const long long ncell = (long long)a.nx * a.ny * a.nz;
     // expand.F90:18-20
+    const float dadt_eps = float(0.5 * sc.dat * sc.dt * sc.rat);  // dadt = 1 - dadt_eps (riemannsolver.F90:36)
     const double afact = sc.dt * (sc.dath / sc.ath);
     const double afact1 = 1.0 / (1.0 + afact);
     const double afact2 = 1.0 / (2.0 + afact);
@@ -226,6 +227,38 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
     // closed forms: 3, 4, 5), so each role holds only its solver's code.
     auto solve_face = [&](auto which, int pattern, int f, int tp, const WsWin& W) {
         const int il = L::fi(f - 1, tp, W.ro), io = L::fi(f, tp, W.ro);
+        // riemannsolver.F90:279-285: the pressure floor of face f
+        auto peak_floor = [&]() -> double {
+            if (AXIS == 0) {
+                // cells f-3 .. f of the pencil, in the reconstruction type
+                // as the reference's R1 gather sees them in this path
+                return peak_value(double(R(S.st[1][L::st(f - 3, tp, W.ro)])),
+                                  double(R(S.st[1][L::st(f - 2, tp, W.ro)])),
+                                  double(R(S.st[1][L::st(f - 1, tp, W.ro)])), double(R(S.st[1][L::st(f, tp, W.ro)])),
+                                  double(R(S.st[2][L::st(f - 2, tp, W.ro)])),
+                                  double(R(S.st[2][L::st(f - 1, tp, W.ro)])), k.dmax);
+            } else if (f < N) {  // the transposed gather, evaluated by the pre-pass
+                return a.peak[pencil_base<AXIS>(W.pid0 + tp, a.nx, a.ny) + stride * f];
+            }
+            return a.peak[ncell + W.pid0 + tp];
+        };
+        if constexpr (Policy::kFaceF32) {
+            // the mixed path's FP32 faces straight from the FP32 rings (the
+            // same arithmetic as the fused sweep's)
+            FaceF lf, rf, of;
+            lf.p = S.ls[0][il]; lf.rho = S.ls[1][il]; lf.u = S.ls[2][il]; lf.v = S.ls[3][il]; lf.w = S.ls[4][il];
+            rf.p = S.rs[0][io]; rf.rho = S.rs[1][io]; rf.u = S.rs[2][io]; rf.v = S.rs[3][io]; rf.w = S.rs[4][io];
+            if (riemann_mixed_f32(pattern, lf, rf, of, k, dadt_eps)) {
+                if (peak_possible) of.p = float(fmax2(double(of.p), peak_floor()));
+                S.rs[0][io] = of.p;
+                S.rs[1][io] = of.rho;
+                S.rs[2][io] = of.u;
+                S.rs[3][io] = of.v;
+                S.rs[4][io] = of.w;
+                return;
+            }
+            if (pattern >= 6) pattern -= 5;  // the FP32 iteration failed: FP64
+        }
         FaceState left, rgt, out;
         left.p = double(S.ls[0][il]);
         left.rho = double(S.ls[1][il]);
@@ -240,21 +273,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
         if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare, decltype(which)::value>(
                 pattern, left, rgt, out, k, sc))
             status |= kStatNewton;
-        if (peak_possible) {  // riemannsolver.F90:279-285
-            double pk;
-            if (AXIS == 0) {
-                // cells f-3 .. f of the pencil, in the reconstruction type
-                // as the reference's R1 gather sees them in this path
-                pk = peak_value(double(R(S.st[1][L::st(f - 3, tp, W.ro)])), double(R(S.st[1][L::st(f - 2, tp, W.ro)])),
-                                double(R(S.st[1][L::st(f - 1, tp, W.ro)])), double(R(S.st[1][L::st(f, tp, W.ro)])),
-                                double(R(S.st[2][L::st(f - 2, tp, W.ro)])), double(R(S.st[2][L::st(f - 1, tp, W.ro)])), k.dmax);
-            } else if (f < N) {  // the transposed gather, evaluated by the pre-pass
-                pk = a.peak[pencil_base<AXIS>(W.pid0 + tp, a.nx, a.ny) + stride * f];
-            } else {
-                pk = a.peak[ncell + W.pid0 + tp];
-            }
-            out.p = fmax2(out.p, pk);
-        }
+        if (peak_possible) out.p = fmax2(out.p, peak_floor());
         S.rs[0][io] = FaceT<Policy>(out.p);
         S.rs[1][io] = FaceT<Policy>(out.rho);
         S.rs[2][io] = FaceT<Policy>(out.u);
