@@ -334,6 +334,7 @@ int hp_init(const hp_params* p, hp_ctx** out) {
             if (fabs(j - rint(j)) < 1e-12 && j >= 1.0 && j <= 9.0) k.jrg = (int)rint(j);
         }
     }
+    hp::set_float_consts(k);
 
     hp::DevCtl& c = *x->ctl_pinned;
     memset(&c, 0, sizeof c);
@@ -794,6 +795,7 @@ int hp_slab_init(hp_ctx* x, int nz_global, int z0) {
     const int nmax = x->box.nx > x->box.ny ? (x->box.nx > nz_global ? x->box.nx : nz_global)
                                            : (x->box.ny > nz_global ? x->box.ny : nz_global);
     x->box.k.dx = 1.0 / (double)nmax;
+    hp::set_float_consts(x->box.k);
     x->box.k.rdx = 1.0 / x->box.k.dx;
     if ((rc = copy_ctl_to_host(x)) != HP_OK) return rc;
     x->ctl_pinned->dx = x->box.k.dx;

@@ -133,6 +133,7 @@ extern "C" int hp_ppmsolver_noalloc(double* p, double* rho, double* vx, double* 
         k.nroot = (int)n;
         if (fabs(j - rint(j)) < 1e-12 && j >= 1.0 && j <= 9.0) k.jrg = (int)rint(j);
     }
+    hp::set_float_consts(k);
 
     hp::StepScalars sc;
     sc.dt = scalars->dt;

@@ -34,6 +34,39 @@ struct Consts {
     int nbound; // ghost layers of the reference's arrays (&MESH nbound): only the
                 // y/z density-peak gather, which indexes those arrays, depends on it
     int pad_;
+    // FP32 copies for the mixed path's FP32 stages (set_float_consts): the
+    // values a conversion in the kernel would give, without the conversion
+    // (kernels under register pressure re-convert a constant at each use)
+    float fgamma, fgamma1, frgamma1, fm, fgf, frm, frgamma, fdx, fflat, fming;
+};
+inline void set_float_consts(Consts& k) {
+    k.fgamma = float(k.gamma);
+    k.fgamma1 = float(k.gamma1);
+    k.frgamma1 = float(k.rgamma1);
+    k.fm = float(k.m);
+    k.fgf = float(k.gf);
+    k.frm = float(k.rm);
+    k.frgamma = float(k.rgamma);
+    k.fdx = float(k.dx);
+    k.fflat = float(k.flatvalue);
+    k.fming = float(k.mingradflat);
+}
+// The constants in type T: the FP64 fields, or their FP32 copies.
+template <class T> struct KT {
+    __device__ __forceinline__ static double gamma(const Consts& k) { return k.gamma; }
+    __device__ __forceinline__ static double gamma1(const Consts& k) { return k.gamma1; }
+    __device__ __forceinline__ static double rgamma1(const Consts& k) { return k.rgamma1; }
+    __device__ __forceinline__ static double dx(const Consts& k) { return k.dx; }
+    __device__ __forceinline__ static double flat(const Consts& k) { return k.flatvalue; }
+    __device__ __forceinline__ static double ming(const Consts& k) { return k.mingradflat; }
+};
+template <> struct KT<float> {
+    __device__ __forceinline__ static float gamma(const Consts& k) { return k.fgamma; }
+    __device__ __forceinline__ static float gamma1(const Consts& k) { return k.fgamma1; }
+    __device__ __forceinline__ static float rgamma1(const Consts& k) { return k.frgamma1; }
+    __device__ __forceinline__ static float dx(const Consts& k) { return k.fdx; }
+    __device__ __forceinline__ static float flat(const Consts& k) { return k.fflat; }
+    __device__ __forceinline__ static float ming(const Consts& k) { return k.fming; }
 };
 struct StepScalars {
     double dt, rdtath, at, dat, rat, ath, dath;
@@ -191,6 +224,9 @@ struct FaceState {
 struct FaceF {
     float p, rho, u, v, w;
 };
+// A face state in the reconstruction type R (the traced states of stage B).
+template <class R> struct FaceOf { using type = FaceState; };
+template <> struct FaceOf<float> { using type = FaceF; };
 
 // Density-peak pressure fix, riemannsolver.F90:279-285.  r1..r4 / u2,u3 are
 // rhobar(1..4) / vxbar(2..3) of the gather (cells f-3..f of the sweep).

@@ -159,7 +159,7 @@ struct PowF32 {
 template <class T, class PowT>
 __device__ __forceinline__ int riemann_classify(T pleft, T pright, T rholeft, T rhoright, T vxleft, T vxright,
                                                 T& cleft, T& cright, const Consts& k) {
-    const T gamma = T(k.gamma);
+    const T gamma = T(KT<T>::gamma(k));
     cleft = sqrt(gamma * pleft / rholeft);
     cright = sqrt(gamma * pright / rhoright);
     T p1, p2, rho1, c1, c2;
@@ -172,7 +172,7 @@ __device__ __forceinline__ int riemann_classify(T pleft, T pright, T rholeft, T 
     const T dv2s = (p2 - p1) / sqrt(T(0.5) * rho1 * ((gamma - T(1)) * p1 + (gamma + T(1)) * p2));
     if (dvv >= dv2s) return 1;
     const T dv1s = -((T(2) * c2 / (gamma - T(1))) * (T(1) - PowT::pm(p1 / p2, k)));
-    const T dv2r = -(T(2) * (c1 + c2) * T(k.rgamma1));
+    const T dv2r = -(T(2) * (c1 + c2) * T(KT<T>::rgamma1(k)));
     if (dvv < dv2s && dvv >= dv1s) return 2;
     if (dvv < dv1s && dvv > dv2r) return 3;
     if (dvv <= dv2r) return 4;
@@ -181,7 +181,7 @@ __device__ __forceinline__ int riemann_classify(T pleft, T pright, T rholeft, T 
 
 // FP32 x^m for the mixed classification.
 struct PowF32m {
-    __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, float(k.m)); }
+    __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, k.fm); }
 };
 
 // ------------------------------------------------------------------------
@@ -207,7 +207,7 @@ struct PowF32m {
 // is not a positive finite number.
 __device__ __forceinline__ float newton_start_f32(float pl, float pr, float rl, float rr, float ul, float ur,
                                                   const Consts& k) {
-    const float g = float(k.gamma), m = float(k.m);
+    const float g = k.fgamma, m = k.fm;
     const float cl = sqrtf(g * pl / rl), cr = sqrtf(g * pr / rr);
     const float q = (cl + cr + (ul - ur) * (g - 1.0f) * 0.5f) / (cl / PowF32::pw(pl, m) + cr / PowF32::pw(pr, m));
     float ps;
@@ -215,7 +215,7 @@ __device__ __forceinline__ float newton_start_f32(float pl, float pr, float rl, 
         const float q2 = q * q;
         ps = q2 * q2 * q;
     } else {
-        ps = PowF32::pw(q, float(k.rm));
+        ps = PowF32::pw(q, k.frm);
     }
     return (ps > 0.0f && ps < 3.0e38f) ? ps : 0.0f;
 }
@@ -340,14 +340,14 @@ __device__ __forceinline__ bool newton_weak(float pl, float pr, float rl, float 
 __device__ __forceinline__ void wave_f32(float x, float pstar, float p, float c, float rc, float sgn, int nroot,
                                          const Consts& k, float& ia, float& vprime) {
     if (pstar >= p) {  // shock: a = c sqrt(gf x + m)
-        ia = rsqrtf(float(k.gf) * x + float(k.m)) * rc;
+        ia = rsqrtf(k.fgf * x + k.fm) * rc;
         const float ca = c * ia;
         vprime = sgn * 0.5f * ia * (1.0f + ca * ca);
     } else {  // rarefaction: a = m c (1 + z + ... + z^(n-1)), z = x^(1/n)
-        const float z = PowF32::pw(x, float(k.m));
+        const float z = PowF32::pw(x, k.fm);
         float s = 1.0f;
         for (int j = 1; j < nroot; ++j) s = fmaf(s, z, 1.0f);
-        ia = rc / (float(k.m) * s);
+        ia = rc / (k.fm * s);
         vprime = sgn * rc * (z / x);
     }
 }
@@ -356,7 +356,7 @@ __device__ __forceinline__ bool riemann_newton_f32(float& pstar, float& vstar, f
                                                    float ul, float ur, const Consts& k) {
     const int n = k.nroot;
     if (n < 2) return false;
-    const float g = float(k.gamma);
+    const float g = k.fgamma;
     const float c2l = g * pl * rl, c2r = g * pr * rr;
     const float rcl = rsqrtf(c2l), rcr = rsqrtf(c2r);
     const float cl = c2l * rcl, cr = c2r * rcr;  // Lagrangian sound speeds
@@ -423,7 +423,7 @@ __device__ __forceinline__ double start_two_shocks(const FaceState& L, const Fac
 template <class S, class FS = FaceState, class O = double>
 __device__ __forceinline__ void sample_two_shocks(const FS& L, const FS& R, O& pm, O& vxm, O& rhom, const Consts& k) {
     const auto pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
-    const S pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
+    const S pmS = S(pm), vxmS = S(vxm), g1 = S(KT<S>::gamma1(k));
     const S rl = S(rholeft), rr = S(rhoright);
     const S rhoshock1 = rhoshock<S>(pmS, S(pleft), rl, g1);
     const S rhoshock2 = rhoshock<S>(pmS, S(pright), rr, g1);
@@ -458,9 +458,8 @@ __device__ __forceinline__ double start_shock_rarefaction(const FaceState& L, co
 template <class S, class PowS, class FS = FaceState, class O = double>
 __device__ __forceinline__ void sample_shock_rarefaction(const FS& L, const FS& R, O cleft, O cright, O& pm, O& vxm,
                                                          O& rhom, const Consts& k) {
-    const double gamma = k.gamma;
     const auto pleft = L.p, pright = R.p, rholeft = L.rho, rhoright = R.rho, vxleft = L.u, vxright = R.u;
-    const S gS = S(gamma), pmS = S(pm), vxmS = S(vxm), g1 = S(k.gamma1);
+    const S gS = S(KT<S>::gamma(k)), pmS = S(pm), vxmS = S(vxm), g1 = S(KT<S>::gamma1(k));
     if (pleft >= pright) {
         const S rr = S(rhoright), rl = S(rholeft);
         const S rhoshock2 = rhoshock<S>(pmS, S(pright), rr, g1);
@@ -507,7 +506,7 @@ template <class T, class PowT>
 __device__ __forceinline__ void riemann_two_rarefactions(T pleft, T pright, T rholeft, T rhoright, T vxleft,
                                                          T vxright, T cleft, T cright, T& pm, T& vxm, T& rhom,
                                                          const Consts& k) {
-    const T gamma = T(k.gamma), rgamma1 = T(k.rgamma1);
+    const T gamma = T(KT<T>::gamma(k)), rgamma1 = T(KT<T>::rgamma1(k));
     const T zeta = (cright / cleft) * PowT::pm(pleft / pright, k);
     const T vtleft = vxleft + T(2) * cleft * rgamma1;
     const T vtright = vxright - T(2) * cright * rgamma1;
@@ -537,7 +536,7 @@ __device__ __forceinline__ void riemann_two_rarefactions(T pleft, T pright, T rh
 
 // FP32 powers of the two-rarefaction form (mixed path).
 struct PowRareF32 {
-    __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, float(k.m)); }
+    __device__ __forceinline__ static float pm(float x, const Consts& k) { return PowF32::pw(x, k.fm); }
     __device__ __forceinline__ static float prm(float x, const Consts& k) {
         if (k.nroot == 5) return x * x * x * x * x;
         if (k.nroot) {
@@ -545,9 +544,9 @@ struct PowRareF32 {
             for (int i = 1; i < k.nroot; ++i) r *= x;
             return r;
         }
-        return PowF32::pw(x, float(k.rm));
+        return PowF32::pw(x, k.frm);
     }
-    __device__ __forceinline__ static float prg(float x, const Consts& k) { return PowF32::pw(x, float(k.rgamma)); }
+    __device__ __forceinline__ static float prg(float x, const Consts& k) { return PowF32::pw(x, k.frgamma); }
 };
 
 // Pattern 4: vacuum, riemannsolver.F90:231-264.
@@ -624,7 +623,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
                 if (pattern == 6) {
                     sample_two_shocks<RareT>(L, R, pm, vxm, rhom, k);
                 } else {
-                    const float g = float(k.gamma);
+                    const float g = k.fgamma;
                     const double cleft = double(sqrtf(g * pl / rl)), cright = double(sqrtf(g * pr / rr));
                     sample_shock_rarefaction<RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
                 }
@@ -642,7 +641,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
                 // Eulerian sound speeds in FP32 (mixed_newton_start forms the
                 // same values); the FP64 ones only when that start fails
                 pm = mixed_newton_start(L.p, R.p, L.rho, R.rho, L.u, R.u, k);
-                const float g = float(k.gamma);
+                const float g = k.fgamma;
                 cleft = double(sqrtf(g * float(L.p) / float(L.rho)));
                 cright = double(sqrtf(g * float(R.p) / float(R.rho)));
                 if (!(pm > 0.0)) {
@@ -662,7 +661,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
         if (pattern == 1) sample_two_shocks<RareT>(L, R, pm, vxm, rhom, k);
         else sample_shock_rarefaction<RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
     } else if (WHICH != kNewtonOnly && pattern == 3) {
-        const RareT g = RareT(k.gamma);
+        const RareT g = RareT(KT<RareT>::gamma(k));
         const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);
         const RareT cleft = sqrt(g * pl / rl), cright = sqrt(g * pr / rr);
         // NaN when no branch of the closed form applies (a NaN state), as
@@ -710,7 +709,7 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
 __device__ __forceinline__ bool riemann_mixed_f32(int pattern, const FaceF& L, const FaceF& R, FaceF& out,
                                                   const Consts& k, float eps) {
     float pm, vxm, rhom;
-    const float g = float(k.gamma);
+    const float g = k.fgamma;
     if (pattern == 3) {
         const float cleft = sqrtf(g * L.p / L.rho), cright = sqrtf(g * R.p / R.rho);
         pm = vxm = rhom = __int_as_float(0x7fc00000);

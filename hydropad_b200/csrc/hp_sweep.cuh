@@ -257,7 +257,8 @@ struct TraceScalars {
 template <class R, bool GRAV, bool PENCIL>
 __device__ __forceinline__ void trace_cell(const R q1[5], const R q2[5], const R q3[5], const R dm[5], const R d0[5],
                                            const R dp[5], R Dm, R Dp, bool fl_any, R g1, R g2, R g3, R gdm, R gd0,
-                                           R gdp, const TraceScalars<R>& ts, R left[5], FaceState& right) {
+                                           R gdp, const TraceScalars<R>& ts, R left[5],
+                                           typename FaceOf<R>::type& right) {
     const R dt_ = ts.dt, rat_ = ts.rat, dat_ = ts.dat, at_ = ts.at, dx_ = ts.dx, gam_ = ts.gam;
     const R flat = fl_any ? ts.flatv : R(0);
     const R pm1 = q1[0], p0 = q2[0], pp1 = q3[0];
@@ -457,7 +458,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     const Consts k = a.k;
     const StepScalars sc = a.ctl->s;
     const R dt_ = R(sc.dt), rat_ = R(sc.rat), dat_ = R(sc.dat), at_ = R(sc.at);
-    const R dx_ = R(k.dx), gam_ = R(k.gamma), flatv_ = R(k.flatvalue), ming_ = R(k.mingradflat);
+    const R dx_ = R(KT<R>::dx(k)), gam_ = R(KT<R>::gamma(k)), flatv_ = R(KT<R>::flat(k)), ming_ = R(KT<R>::ming(k));
     const TraceScalars<R> ts{dt_, rat_, dat_, at_, dx_, gam_, flatv_};
     if (a.ctl->done) return;  // told >= tstop: the time loop has ended (main.F90:100)
 
@@ -485,7 +486,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     unsigned long long kmin = kKeyPosInf, kmax = 0ULL, kvel = 0ULL;
     unsigned status = 0;
 
-    FaceState right;        // right state of face c (cell c), from stage B
+    typename FaceOf<R>::type right;  // right state of face c (cell c), from stage B, in the type R
 
     // Barriers.  Stages load, A, B and C1 exchange data only along a pencil
     // (ring neighbours e-2 .. e+2).  Along x a warp holds whole pencil

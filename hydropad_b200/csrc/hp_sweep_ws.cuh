@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
     const Consts k = a.k;
     const StepScalars sc = a.ctl->s;
     const R dt_ = R(sc.dt), rat_ = R(sc.rat), dat_ = R(sc.dat), at_ = R(sc.at);
-    const R dx_ = R(k.dx), gam_ = R(k.gamma), flatv_ = R(k.flatvalue), ming_ = R(k.mingradflat);
+    const R dx_ = R(KT<R>::dx(k)), gam_ = R(KT<R>::gamma(k)), flatv_ = R(KT<R>::flat(k)), ming_ = R(KT<R>::ming(k));
     const TraceScalars<R> ts{dt_, rat_, dat_, at_, dx_, gam_, flatv_};
     const double rmin0 = dkey_decode(a.ctl->rho_key[a.bslot][0]);
     const double rmax0 = dkey_decode(a.ctl->rho_key[a.bslot][1]);
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(WsLayout<AXIS, P, T, NW>::kThreads, MINB)
                 }
                 __syncwarp();
                 // ---------------- B: cell c = ew-3 ----------------
-                FaceState right;
+                typename FaceOf<R>::type right;
                 {
                     const int c = ew - 3;
                     if (activew && c >= -1 && c <= N) {
