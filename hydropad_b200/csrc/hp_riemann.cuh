@@ -605,14 +605,18 @@ __device__ __forceinline__ int solver_pattern(int pattern, float pl, float pr, f
 // (kClosedOnly), for a caller that only ever sees those (the same
 // arithmetic, less code).  Patterns 6 and 7 (mixed path only) are the weak
 // faces of patterns 1 and 2: their p*, u* come from the FP32 iteration, or,
-// if it fails, from the FP64 one as for patterns 1 and 2.
-enum { kAllPatterns = 0, kNewtonOnly = 1, kClosedOnly = 2 };
+// if it fails, from the FP64 one as for patterns 1 and 2.  kFallback (mixed
+// path, after riemann_mixed_f32 declined the face) holds the FP64 code
+// alone: patterns 1, 2, 4, 5, and pattern 3 straight to its FP64 solution
+// (the FP32 closed form is known to have failed); the FP32 branches, which
+// the caller has already run, stay out of the kernel's instruction stream.
+enum { kAllPatterns = 0, kNewtonOnly = 1, kClosedOnly = 2, kFallback = 3 };
 template <class Pow, class RareT, class PowRare, int WHICH = kAllPatterns>
 __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState& L, const FaceState& R,
                                                    FaceState& out, const Consts& k, const StepScalars& s) {
     double pm = __longlong_as_double(0x7ff8000000000000ULL), vxm = pm, rhom = pm;
     bool ok = true;
-    if constexpr (Pow::kShortNewton && WHICH != kClosedOnly) {
+    if constexpr (Pow::kShortNewton && WHICH != kClosedOnly && WHICH != kFallback) {
         if (pattern == 6 || pattern == 7) {
             const float pl = float(L.p), pr = float(R.p), rl = float(L.rho), rr = float(R.rho);
             const float ul = float(L.u), ur = float(R.u);
@@ -660,6 +664,13 @@ __device__ __forceinline__ bool riemann_by_pattern(int pattern, const FaceState&
         ok = riemann_newton<Pow>(pm, vxm, L.p, R.p, L.rho, R.rho, L.u, R.u, k);
         if (pattern == 1) sample_two_shocks<RareT>(L, R, pm, vxm, rhom, k);
         else sample_shock_rarefaction<RareT, PowRare>(L, R, cleft, cright, pm, vxm, rhom, k);
+    } else if (WHICH == kFallback && pattern == 3) {
+        // a face at the edge of the vacuum condition: classified and solved
+        // again in FP64, as below
+        double cl, cr;
+        const int p64 = riemann_classify<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cl, cr, k);
+        if (p64 == 4) riemann_vacuum(L, R, cl, cr, pm, vxm, rhom, k);
+        else riemann_two_rarefactions<double, Pow>(L.p, R.p, L.rho, R.rho, L.u, R.u, cl, cr, pm, vxm, rhom, k);
     } else if (WHICH != kNewtonOnly && pattern == 3) {
         const RareT g = RareT(KT<RareT>::gamma(k));
         const RareT pl = RareT(L.p), pr = RareT(R.p), rl = RareT(L.rho), rr = RareT(R.rho);

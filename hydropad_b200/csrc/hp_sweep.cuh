@@ -771,7 +771,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 rgt.u = S.rs[2][io];
                 rgt.v = S.rs[3][io];
                 rgt.w = S.rs[4][io];
-                if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare>(
+                constexpr int kWhich = Policy::kFaceF32 ? kFallback : kAllPatterns;
+                if (!riemann_by_pattern<Pow, typename Policy::RareT, typename Policy::PowRare, kWhich>(
                         pattern, left, rgt, out, k, sc))
                     status |= kStatNewton;
                 if (peak_possible) out.p = fmax2(out.p, peak_floor());
