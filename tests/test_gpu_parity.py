@@ -1,6 +1,6 @@
 """GPU parity: the fused CUDA sweeps against the CPU oracle, through the C ABI.
 
-FP64 gate (north star): relative L1 <= 1e-10 per field after 10 steps; in
+FP64 gate: relative L1 <= 1e-10 per field after 10 steps; in
 practice the FP64 path is compiled without FMA contraction and agrees with
 the oracle to a few ulp.  Mixed precision: density relative L1 <= 1e-5.
 """
@@ -290,7 +290,7 @@ def test_config1_sod64(oracle):
 
 def test_config2_eds256_fp64_ten_steps(oracle):
     """The cosmological configuration at its full size (256^3): ten steps of
-    the FP64 path against the oracle, the north star's FP64 gate."""
+    the FP64 path against the oracle at the FP64 gate (1e-10 per field)."""
     n = 256
     state = grf_state(n, seed=12345)
     prm = params_for((n, n, n), cosmo=True)
