@@ -257,7 +257,7 @@ const char* hp_strerror(int code) {
         case HP_ERR_NOT_ATTACHED: return "no state attached";
         case HP_ERR_STATE_MISMATCH: return "host arrays are not the attached state";
         case HP_ERR_NO_DEVICE: return "no usable sm_100 CUDA device";
-        case HP_ERR_UNSUPPORTED: return "not supported by this build (the density-peak fix across z slabs)";
+        case HP_ERR_UNSUPPORTED: return "not supported by this library (the density-peak fix across z slabs)";
         case HP_ERR_TIMEOUT: return "a bounded wait of the pipelined sweep gave up (results void)";
     }
     return "unknown error";

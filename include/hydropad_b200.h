@@ -48,7 +48,7 @@ enum {
     HP_ERR_NOT_ATTACHED = -7,  /* sweep requested before hp_attach_state */
     HP_ERR_STATE_MISMATCH = -8,/* host arrays differ from the attached ones */
     HP_ERR_NO_DEVICE = -9,     /* no CUDA device / wrong architecture */
-    HP_ERR_UNSUPPORTED = -10,  /* a case this build does not take (the density-peak fix across z slabs) */
+    HP_ERR_UNSUPPORTED = -10,  /* a case this library does not take (the density-peak fix across z slabs) */
     HP_ERR_TIMEOUT = -11       /* a bounded wait inside the pipelined sweep gave up; the sweep's
                                   results are void (no counterpart in the reference) */
 };
