@@ -198,7 +198,7 @@ struct SweepSmem {
     R st[5][kC];                // state ring: p, rho, u, v, w (FP32 copy in the mixed path)
     double sg[kG];              // gravity ring: g = -gforce of this sweep's axis
     R slg[kG];                  // ajside slope of g
-    R sl[5][kC];                // ajside slopes
+    alignas(8) R sl[5][kC];     // ajside slopes (after the walk: the block reduction's buffer)
     R d2[kC];                   // dda second difference of rho
     unsigned char pf[kC];       // flattening flag of pair (c, c+1)
     R ls[5][kC];                // traced left state (face c+1) from cell c
@@ -206,12 +206,22 @@ struct SweepSmem {
     // Riemann state of face f (FaceT): each slot is read and then written by
     // the one thread that solves that face
     FaceT<Policy> rs[5][kC];
-    unsigned short work[kBuckets][P * T];  // Riemann problems of the iteration (by the thread
-                                           // index that classified them), in buckets
+    // Riemann problems of the iteration (by the thread index that classified
+    // them, a byte when the CTA has at most 256 threads), in buckets
+    typename std::conditional<(P * T <= 256), unsigned char, unsigned short>::type work[kBuckets][P * T];
     int bcnt[2][kBuckets];      // bucket fill counts (alternate iterations use alternate rows)
     R sv[5][3 * P];             // original values of cells 0..2 (they only refill the state ring)
-    unsigned long long red[128];
 };
+
+// The block reduction at the end of a walk (block_flush, 4 x 32 words)
+// reuses the slope ring: block_flush starts with a CTA barrier, after which
+// no thread reads the ring again in this walk, and the next walk of the
+// batched kernel writes it only after its own CTA barriers.
+template <class Smem>
+__device__ __forceinline__ unsigned long long* red_buffer(Smem& S) {
+    static_assert(sizeof(S.sl) >= 128 * sizeof(unsigned long long), "reduction buffer");
+    return reinterpret_cast<unsigned long long*>(&S.sl[0][0]);
+}
 
 // Barrier between stages that pass data along the pencil only: a warp
 // barrier when every warp holds whole pencil windows, else the CTA's.
@@ -683,7 +693,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
             int off = 0;
             if (bucket && lane == leader) off = atomicAdd(&S.bcnt[par][bucket - 1], __popc(peers));
             off = __shfl_sync(0xffffffffu, off, leader);
-            if (bucket) S.work[bucket - 1][off + __popc(peers & ((1u << lane) - 1u))] = (unsigned short)tid;
+            if (bucket) S.work[bucket - 1][off + __popc(peers & ((1u << lane) - 1u))] = tid;
         }
         __syncthreads();
         // C2: solve problem number tid of the buckets laid end to end.
@@ -850,7 +860,7 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     }
     block_flush(kmin, kmax, kvel, status, &a.ctl->rho_key[(a.bslot + 1) % 3][0],
                 &a.ctl->rho_key[(a.bslot + 1) % 3][1], (a.flags & kFlagSpeed) ? &a.ctl->velmax_key : nullptr,
-                &a.ctl->status, S.red);
+                &a.ctl->status, red_buffer(S));
 }
 
 // One box per launch: CTA b takes pencils b*P .. b*P+P-1.
