@@ -54,7 +54,8 @@ enum {
 };
 
 /* HP_PREC_FP64: every stage in FP64, the reference's arithmetic operation by
- * operation (within 1e-10 relative L1 of the reference after 10 steps).
+ * operation (within 1e-10 relative L1 per field, after 10 steps, of a CPU
+ * restatement of the reference's algorithm).
  * HP_PREC_MIXED: reconstruction, tracing, classification, the closed-form
  * Riemann solutions and the Newton iteration of weak faces (pressures
  * within a factor 4, velocity jump at most cL + cR) in FP32; the Newton
