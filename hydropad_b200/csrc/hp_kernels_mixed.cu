@@ -1,9 +1,11 @@
 // hp_kernels_mixed.cu -- mixed-precision sweep instantiations.
 //
-// Reconstruction, flattening, characteristic tracing and the traced face
-// states run in FP32; the Riemann solver (Newton for p*, u*), the
-// conservative update and the total-minus-kinetic energy of the dual-energy
-// switch stay FP64, and the state in HBM stays FP64.
+// Reconstruction, flattening, characteristic tracing, the traced face
+// states, the closed-form Riemann solutions and the Newton iteration of
+// weak faces run in FP32; the Newton iteration for p*, u* across strong
+// shocks and near-vacuum states, the conservative update (fluxes formed in
+// FP64) and the total-minus-kinetic energy of the dual-energy switch stay
+// FP64, and the state in HBM stays FP64.
 #include <cuda_runtime.h>
 
 #include "hp_device.cuh"

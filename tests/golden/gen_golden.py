@@ -257,6 +257,29 @@ def riemann(pstar, pl, pr, rl, rr, ul, ur, S):
     return pstar, vstar
 
 
+# Faces per wave pattern of the last generated case: two shocks, shock +
+# rarefaction, two rarefactions, vacuum (the branch order below), then the
+# two-shock and shock + rarefaction faces that are strong (a pressure jump
+# above 100 or streams colliding faster than cL + cR).
+TALLY = [0] * 6
+
+
+def _tally(dvv, dv2s, dv1s, dv2r, p1, p2, csum):
+    if dvv >= dv2s:
+        pat = 0
+    elif dvv >= dv1s:
+        pat = 1
+    elif dvv > dv2r:
+        pat = 2
+    elif dvv <= dv2r:
+        pat = 3
+    else:
+        return
+    TALLY[pat] += 1
+    if pat < 2 and (p2 > 100.0 * p1 or dvv > csum):
+        TALLY[4 + pat] += 1
+
+
 def riemannsolver(rhobar, vxbar, pl, pr, rl, rr, ul, ur, vl, vr, wl, wr, S):
     g = S.gamma
     cleft = np.sqrt(g * pl / rl)
@@ -270,6 +293,7 @@ def riemannsolver(rhobar, vxbar, pl, pr, rl, rr, ul, ur, vl, vr, wl, wr, S):
     dv2s = (p2 - p1) / np.sqrt(0.50 * rho1 * ((g - 1) * p1 + (g + 1) * p2))
     dv1s = -((2.0 * c2 / (g - 1.0)) * (1.0 - (p1 / p2) ** S.m))
     dv2r = -(2.0 * (c1 + c2) * S.rgamma1)
+    _tally(dvv, dv2s, dv1s, dv2r, p1, p2, cleft + cright)
     pm = vxm = rhom = float("nan")
     if dvv >= dv2s:
         pm, vxm = riemann(MAX(pl, pr), pl, pr, rl, rr, ul, ur, S)
@@ -672,6 +696,26 @@ def make_case(seed, n=(10, 8, 6), nb=3, peak=False, single=False):
     return [_ghost(a, nb) for a in (p, rho, *vel)]
 
 
+def make_extreme(seed, n, axis, nb=3):
+    """Strong waves along the sweep axis: blocks of 3 cells cycle through
+    cold gas (p ~ 1e-2), dense gas (rho ~ 100) and hot gas (p ~ 1e3), and
+    the sweep velocity flips between +0.5 and -0.5 (about 4 cold sound
+    speeds) every 3 cells, offset from the blocks: streams collide (strong
+    two-shock faces), recede (vacuum faces) and meet pressure jumps of 1e5
+    (strong shock + rarefaction faces)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shape = tuple(n)
+    i = np.arange(shape[axis])
+    sh = [1, 1, 1]
+    sh[axis] = shape[axis]
+    blk = ((i // 3) % 4).reshape(sh)
+    rho = np.where(blk == 1, 100.0, 1.0) * (1.0 + 0.2 * rng.random(shape))
+    p = np.where(blk == 2, 1e3, 1e-2) * (1.0 + 0.2 * rng.random(shape))
+    vel = [0.05 * rng.standard_normal(shape) for _ in range(3)]
+    vel[axis] = vel[axis] + np.where(((i + 1) // 3) % 2 == 0, 0.5, -0.5).reshape(sh)
+    return [_ghost(a, nb) for a in (p, rho, *vel)]
+
+
 CASES = [
     # name, seed, shape, sweep, scalars, peak
     ("static_x", 1, (10, 8, 6), 1, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
@@ -691,6 +735,10 @@ CASES = [
     ("pencil_y", 11, (8, 10, 6), 2, dict(dt=1.5e-3, at=0.05, dat=3.1, ath=0.0502), dict()),
     ("pencil_z", 12, (6, 8, 10), 3, dict(dt=2e-3, at=1.0, dat=0.0, ath=1.0), dict()),
     ("pencil_peak_x", 13, (10, 8, 6), 1, dict(dt=1e-3, at=1.0, dat=0.0, ath=1.0), dict(dmax=2.0)),
+    # strong shocks, vacuum and two-rarefaction faces (make_extreme); dt at a
+    # Courant number of about 0.32
+    ("extreme_x", 7, (12, 8, 8), 1, dict(dt=6e-4, at=1.0, dat=0.0, ath=1.0), dict()),
+    ("extreme_z", 8, (8, 8, 12), 3, dict(dt=3e-5, at=0.05, dat=3.1, ath=0.0502), dict()),
 ]
 
 
@@ -709,15 +757,22 @@ def gravity_field(shape, nb, alpha=40.0, sigma=0.3):
 
 def run_case(name, seed, shape, nd, tsc, extra):
     nb = 3
-    F = make_case(seed, shape, nb, peak="peak" in name, single=name == "pencil_peak_x")
+    if name.startswith("extreme"):
+        F = make_extreme(seed, shape, nd - 1, nb)
+    else:
+        F = make_case(seed, shape, nb, peak="peak" in name, single=name == "pencil_peak_x")
     S = Sc(5.0 / 3.0, 1.0 / max(shape), **tsc, **extra)
     G = gravity_field(shape, nb) if name.startswith("grav") else None
     if name.startswith("pencil"):
         rng = np.random.Generator(np.random.PCG64(seed + 100))
         cho = _ghost(rng.integers(0, 3, shape).astype(np.float64), nb)
         return F, ppmsolver_pencil(F, nb, nd, S, cho), S, {"cho": cho}
+    TALLY[:] = [0] * len(TALLY)
     out = ppmsolver(F, nb, nd, S, G)
-    return F, out, S, ({} if G is None else {"gforce": G})
+    more = {} if G is None else {"gforce": G}
+    if name.startswith("extreme"):
+        more["patterns"] = np.array(TALLY)
+    return F, out, S, more
 
 
 def main(names=None):

@@ -53,7 +53,7 @@ def test_oracle_matches_golden(oracle, name):
 
 
 def test_golden_set_present():
-    assert len(GOLDEN) >= 13, "run tests/golden/gen_golden.py"
+    assert len(GOLDEN) >= 15, "run tests/golden/gen_golden.py"
 
 
 def test_pencil_peak_case_exercises_the_peaks():
@@ -84,3 +84,15 @@ def test_peak_case_exercises_the_fix():
     r = rho
     hit = (r[1:-2] > dmax * r[:-3]) & (r[2:-1] > dmax * r[3:])
     assert hit.any()
+
+
+@pytest.mark.parametrize("name", ["extreme_x", "extreme_z"])
+def test_extreme_cases_reach_every_pattern(name):
+    """The extreme cases must pin the oracle on every wave pattern of
+    riemannsolver.F90 (two shocks, shock + rarefaction, two rarefactions,
+    vacuum), strong shocks included: the generator's tally of the faces."""
+    z, _, out = load_case(name)
+    two_shocks, shock_rare, two_rare, vacuum, strong_2s, strong_sr = (int(v) for v in z["patterns"])
+    assert min(two_shocks, shock_rare, two_rare, vacuum) > 0, z["patterns"]
+    assert strong_2s > 0 and strong_sr > 0, z["patterns"]
+    assert all(np.isfinite(a).all() for a in out)
