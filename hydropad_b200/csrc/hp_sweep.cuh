@@ -161,30 +161,46 @@ struct SweepLayout {
 };
 
 // Buckets of the Riemann problems, in the order the solving threads take
-// them: shock + rarefaction with the rarefaction on the left (pL >= pR),
-// two shocks, shock + rarefaction with the rarefaction on the right (FP64
-// Newton), then, in the mixed path (W), the same three for the weak faces
-// (FP32 Newton, patterns 7, 6, 7), then the closed forms.  The Newton
-// buckets of one precision share the iteration, and neighbouring buckets
-// differ in the wave on one side only, so a warp that straddles two of
-// them diverges on one side of the loop body.
+// them.  FP64 path: shock + rarefaction with the rarefaction on the left
+// (pL >= pR), two shocks, shock + rarefaction with the rarefaction on the
+// right (Newton), then the closed forms (patterns 3, 4, 5).  Mixed path
+// (W): the weak faces' three (FP32 Newton, patterns 7, 6, 7), the closed
+// forms, then the strong faces' three (FP64 Newton, patterns 2, 1, 2): the
+// warp that holds the few strong faces of an iteration then shares it with
+// closed forms, not with FP32 Newton faces, and the longest warp of the
+// stage (run one after the other where a warp holds both) gets shorter.
+// The Newton buckets of one precision share the iteration, and neighbouring
+// Newton buckets differ in the wave on one side only, so a warp that
+// straddles two of them diverges on one side of the loop body.
 template <bool W> constexpr int kBucketsOf = W ? 9 : 6;
 // 1 + bucket of a face of pattern 1..7 (patterns 2, 7: rare_left = pL >= pR)
 template <bool W>
 __device__ __forceinline__ int bucket_of(int pattern, bool rare_left) {
-    if (pattern == 2) return rare_left ? 1 : 3;
-    if (pattern == 1) return 2;
-    if (pattern == 7) return rare_left ? 4 : 6;
-    if (pattern == 6) return 5;
-    return W ? pattern + 4 : pattern + 1;
+    if constexpr (W) {
+        if (pattern == 7) return rare_left ? 1 : 3;
+        if (pattern == 6) return 2;
+        if (pattern == 2) return rare_left ? 7 : 9;
+        if (pattern == 1) return 8;
+        return pattern + 1;  // 3, 4, 5 -> 4, 5, 6
+    } else {
+        if (pattern == 2) return rare_left ? 1 : 3;
+        if (pattern == 1) return 2;
+        return pattern + 1;
+    }
 }
 template <bool W>
 __device__ __forceinline__ int pattern_of_bucket(int c) {
-    if (c == 0 || c == 2) return 2;
-    if (c == 1) return 1;
-    if (W && (c == 3 || c == 5)) return 7;
-    if (W && c == 4) return 6;
-    return W ? c - 3 : c;
+    if constexpr (W) {
+        if (c == 0 || c == 2) return 7;
+        if (c == 1) return 6;
+        if (c == 6 || c == 8) return 2;
+        if (c == 7) return 1;
+        return c;  // 3, 4, 5
+    } else {
+        if (c == 0 || c == 2) return 2;
+        if (c == 1) return 1;
+        return c;
+    }
 }
 
 template <int AXIS, int P, int T, int RING, class Policy, bool GRAV = false, bool PENCIL = false>
