@@ -526,13 +526,28 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
     // path's D reads the cell from global memory instead, so its y/z sweeps
     // need no barrier there (everything else the load writes is read after
     // the next barrier only).
+    // Early load (the mixed path's z sweeps): the cells of the next
+    // iteration are loaded by each thread as soon as its C2 work is done,
+    // before the C2 -> D barrier, which then also publishes them to the
+    // layout of stages A-C1.  The threads that finish C2 early load while
+    // the Newton faces are still being solved, and the barrier after the
+    // load goes.  It needs D to leave the state ring alone (the load then
+    // overwrites slots of cells D of this iteration would read) and C2 not
+    // to read it (the x sweep's density-peak window does; y/z read the
+    // pre-pass's values).  Measured on a late 512^3 state (tile 7): z
+    // sweeps 7.76 -> 7.58 ms, whose loads are a plane apart and take the
+    // longest; y sweeps 7.58 -> 7.65 ms (the load's registers in the C2
+    // region add spills), so y keeps the load at the top.  The load of a wrapped cell e >= N keeps its rule:
+    // it reads the save area (written by an earlier load) when D of the
+    // iteration before e's could have overwritten cell e-N, which with the
+    // early load may not have run yet; either copy holds the original value.
     constexpr bool kWarpPencils = AXIS == 0 && T <= 32 && (32 % T) == 0;
     constexpr bool kWarpStages = kWarpPencils || L::kYZWarp;  // A -> B -> C1 within a warp
     constexpr bool kDReadsRing = sizeof(R) == sizeof(double) || GRAV;
+    constexpr bool kEarlyLoad = AXIS == 2 && !kDReadsRing && !PENCIL;
     constexpr bool kW = Policy::kWeakNewton;
     constexpr int kBuckets = kBucketsOf<kW>;
     if (tid < 2 * kBuckets) S.bcnt[tid / kBuckets][tid % kBuckets] = 0;
-    __syncthreads();
     int par = 0;  // row of bcnt of this iteration
 
     using DivD = typename Policy::DivD;
@@ -567,12 +582,8 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                                                   status);
     };
 
-    for (int b = -4; b <= N + 3 + kLag; b += T, par ^= 1) {
-        const int e = b + tl;    // load and update layout
-        const int ew = b + tlw;  // layout of stages A, B and C1
-        if constexpr (kWarpPencils) __syncwarp();
-        else if constexpr (kDReadsRing) __syncthreads();
-        // ---------------- load cell e ----------------
+    // ---------------- load: cell e of this thread's pencil (load layout) ----------------
+    auto load_cell = [&](const int e) {
         if (active && e >= -4 && e <= N + 2) {
             double v[5];
             // Cell e-N (0..2) is overwritten by stage D of the iteration that
@@ -621,7 +632,19 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 S.sg[ix] = -a.g[base + stride * s];
             }
         }
-        pencil_sync<kWarpPencils>();  // y/z: the threads change layout here
+    };
+
+    if constexpr (kEarlyLoad) load_cell(-4 + tl);
+    __syncthreads();
+    for (int b = -4; b <= N + 3 + kLag; b += T, par ^= 1) {
+        const int e = b + tl;    // load and update layout
+        const int ew = b + tlw;  // layout of stages A, B and C1
+        if constexpr (!kEarlyLoad) {
+            if constexpr (kWarpPencils) __syncwarp();
+            else if constexpr (kDReadsRing) __syncthreads();
+            load_cell(e);
+            pencil_sync<kWarpPencils>();  // y/z: the threads change layout here
+        }
         // ---------------- A: cell c = e-1 ----------------
         {
             const int c = ew - 1;
@@ -808,6 +831,9 @@ __device__ __forceinline__ void sweep_pencils(const SweepArgs& a, long long pid0
                 S.rs[3][io] = FaceT<Policy>(out.v);
                 S.rs[4][io] = FaceT<Policy>(out.w);
             }
+        }
+        if constexpr (kEarlyLoad) {
+            if (b + T <= N + 3 + kLag) load_cell(e + T);  // the next iteration's cell
         }
         __syncthreads();
         // ---------------- D: cell d = e-4 ----------------
