@@ -739,6 +739,7 @@ CASES = [
     # Courant number of about 0.32
     ("extreme_x", 7, (12, 8, 8), 1, dict(dt=6e-4, at=1.0, dat=0.0, ath=1.0), dict()),
     ("extreme_z", 8, (8, 8, 12), 3, dict(dt=3e-5, at=0.05, dat=3.1, ath=0.0502), dict()),
+    ("extreme_y", 9, (8, 12, 8), 2, dict(dt=6e-4, at=1.0, dat=0.0, ath=1.0), dict()),
 ]
 
 

@@ -29,7 +29,7 @@ MIXED_TOL = 1e-4
 FIELDS = ("p", "rho", "vx", "vy", "vz")
 
 
-@pytest.mark.parametrize("name", ["extreme_x", "extreme_z"])
+@pytest.mark.parametrize("name", ["extreme_x", "extreme_y", "extreme_z"])
 def test_extreme_golden_sweep(oracle, name):
     """One sweep of the golden extreme case (the generator's own time
     scalars) against the second restatement's output."""

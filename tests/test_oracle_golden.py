@@ -53,7 +53,7 @@ def test_oracle_matches_golden(oracle, name):
 
 
 def test_golden_set_present():
-    assert len(GOLDEN) >= 15, "run tests/golden/gen_golden.py"
+    assert len(GOLDEN) >= 16, "run tests/golden/gen_golden.py"
 
 
 def test_pencil_peak_case_exercises_the_peaks():
@@ -86,7 +86,7 @@ def test_peak_case_exercises_the_fix():
     assert hit.any()
 
 
-@pytest.mark.parametrize("name", ["extreme_x", "extreme_z"])
+@pytest.mark.parametrize("name", ["extreme_x", "extreme_y", "extreme_z"])
 def test_extreme_cases_reach_every_pattern(name):
     """The extreme cases must pin the oracle on every wave pattern of
     riemannsolver.F90 (two shocks, shock + rarefaction, two rarefactions,
