@@ -389,6 +389,13 @@ def riemannsolver(rhobar, vxbar, pl, pr, rl, rr, ul, ur, vl, vr, wl, wr, S):
     return pm, rhom, vxm, vym, vzm
 
 
+# Cells per dual-energy branch of the last generated case: the new internal
+# energy from total minus kinetic (eeaux / etot >= eta2), the pressure from
+# it (eta1 <= ratio < eta2), the pressure from the separately advected
+# internal energy (ratio < eta1).
+DUAL = [0] * 3
+
+
 def integrate(f1, f2, pres, rho, vx, vy, vz, etot, eint, ghalf, S):
     pm1, rhom1, vxm1, vym1, vzm1 = f1
     pm2, rhom2, vxm2, vym2, vzm2 = f2
@@ -417,6 +424,7 @@ def integrate(f1, f2, pres, rho, vx, vy, vz, etot, eint, ghalf, S):
     if eeaux / etotnew >= S.eta2:
         eintnew = eeaux
     pnew = (g - 1) * eeaux if eeaux / etotnew >= S.eta1 else (g - 1) * eintnew
+    DUAL[0 if eeaux / etotnew >= S.eta2 else (1 if eeaux / etotnew >= S.eta1 else 2)] += 1
     if eintnew <= 0.0:
         pnew = pres
     if rhonew <= 0.:
@@ -696,6 +704,19 @@ def make_case(seed, n=(10, 8, 6), nb=3, peak=False, single=False):
     return [_ghost(a, nb) for a in (p, rho, *vel)]
 
 
+def make_cold(seed, n, nb=3):
+    """Cold, fast gas (p ~ 1e-6, sound speed ~ 1.3e-3): velocities of random
+    sign whose magnitude spans 1e-3 .. 1 cell by cell, so the ratio of
+    internal to total energy spans every branch of the dual-energy switch
+    (integrate.F90), down to Mach numbers of several hundred."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    shape = tuple(n)
+    rho = 1.0 + 0.5 * rng.random(shape)
+    p = 1e-6 * (1.0 + rng.random(shape))
+    vel = [rng.standard_normal(shape) * 10.0 ** rng.uniform(-3.0, 0.0, shape) for _ in range(3)]
+    return [_ghost(a, nb) for a in (p, rho, *vel)]
+
+
 def make_extreme(seed, n, axis, nb=3):
     """Strong waves along the sweep axis: blocks of 3 cells cycle through
     cold gas (p ~ 1e-2), dense gas (rho ~ 100) and hot gas (p ~ 1e3), and
@@ -740,6 +761,10 @@ CASES = [
     ("extreme_x", 7, (12, 8, 8), 1, dict(dt=6e-4, at=1.0, dat=0.0, ath=1.0), dict()),
     ("extreme_z", 8, (8, 8, 12), 3, dict(dt=3e-5, at=0.05, dat=3.1, ath=0.0502), dict()),
     ("extreme_y", 9, (8, 12, 8), 2, dict(dt=6e-4, at=1.0, dat=0.0, ath=1.0), dict()),
+    # cold, fast gas over every branch of the dual-energy switch (make_cold);
+    # Courant numbers about 0.2
+    ("cold_x", 14, (10, 8, 8), 1, dict(dt=1e-2, at=1.0, dat=0.0, ath=1.0), dict()),
+    ("cold_z", 15, (8, 8, 10), 3, dict(dt=5e-4, at=0.05, dat=3.1, ath=0.0502), dict()),
 ]
 
 
@@ -760,6 +785,8 @@ def run_case(name, seed, shape, nd, tsc, extra):
     nb = 3
     if name.startswith("extreme"):
         F = make_extreme(seed, shape, nd - 1, nb)
+    elif name.startswith("cold"):
+        F = make_cold(seed, shape, nb)
     else:
         F = make_case(seed, shape, nb, peak="peak" in name, single=name == "pencil_peak_x")
     S = Sc(5.0 / 3.0, 1.0 / max(shape), **tsc, **extra)
@@ -769,10 +796,13 @@ def run_case(name, seed, shape, nd, tsc, extra):
         cho = _ghost(rng.integers(0, 3, shape).astype(np.float64), nb)
         return F, ppmsolver_pencil(F, nb, nd, S, cho), S, {"cho": cho}
     TALLY[:] = [0] * len(TALLY)
+    DUAL[:] = [0] * len(DUAL)
     out = ppmsolver(F, nb, nd, S, G)
     more = {} if G is None else {"gforce": G}
     if name.startswith("extreme"):
         more["patterns"] = np.array(TALLY)
+    if name.startswith("cold"):
+        more["dual"] = np.array(DUAL)
     return F, out, S, more
 
 

@@ -53,7 +53,7 @@ def test_oracle_matches_golden(oracle, name):
 
 
 def test_golden_set_present():
-    assert len(GOLDEN) >= 16, "run tests/golden/gen_golden.py"
+    assert len(GOLDEN) >= 18, "run tests/golden/gen_golden.py"
 
 
 def test_pencil_peak_case_exercises_the_peaks():
@@ -95,4 +95,15 @@ def test_extreme_cases_reach_every_pattern(name):
     two_shocks, shock_rare, two_rare, vacuum, strong_2s, strong_sr = (int(v) for v in z["patterns"])
     assert min(two_shocks, shock_rare, two_rare, vacuum) > 0, z["patterns"]
     assert strong_2s > 0 and strong_sr > 0, z["patterns"]
+    assert all(np.isfinite(a).all() for a in out)
+
+
+@pytest.mark.parametrize("name", ["cold_x", "cold_z"])
+def test_cold_cases_reach_every_dual_energy_branch(name):
+    """The cold cases must pin the oracle on every branch of the dual-energy
+    switch of integrate.F90: internal energy replaced by total minus kinetic,
+    pressure from total minus kinetic, pressure from the advected internal
+    energy (the generator's tally of the cells)."""
+    z, _, out = load_case(name)
+    assert all(int(v) > 0 for v in z["dual"]), z["dual"]
     assert all(np.isfinite(a).all() for a in out)
